@@ -1,0 +1,581 @@
+// alto_engine.cu -- the engine object and the per-batch C ABI (alto_engine_new / alto_answer and friends).
+//
+// Per batch the host settles statuses 1 and 2 from the frame lengths and headers, copies the remaining frames
+// into device staging slots, and enqueues on the engine's stream:
+//   validate (statuses 0/2/3) -> limb split of query and key words -> scan GEMM -> pack GEMM -> tail.
+// The statuses come back early through a pinned buffer while the GEMMs run; the host then queues the copies of the
+// valid responses only, so rejected output buffers are never touched.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/altopir_gpu.h"
+#include "kernels.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+void set_error(const char *where, cudaError_t e) {
+  g_last_error = std::string(where) + ": " + cudaGetErrorString(e);
+}
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+#define ALTO_CK(call)                 \
+  do {                                \
+    cudaError_t e_ = (call);          \
+    if (e_ != cudaSuccess) {          \
+      set_error(#call, e_);           \
+      return false;                   \
+    }                                 \
+  } while (0)
+
+constexpr size_t kSlotLead = 7;  // frame offset inside a staging slot: puts the key words on a 16-byte boundary
+
+// ------------------------------------------------------------------------------------------- tensor maps
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// A row-major u8 matrix of `outer` rows x `inner` bytes (row stride `stride`), read in boxes of 128 bytes x
+// box_rows rows with 128-byte swizzling; out-of-range parts of a box read as zero.
+bool make_map(CUtensorMap *m, const void *base, uint64_t inner, uint64_t outer, uint64_t stride, uint32_t box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) {
+    set_error("cuTensorMapEncodeTiled is unavailable");
+    return false;
+  }
+  const cuuint64_t dims[2] = {inner, outer};
+  const cuuint64_t strides[1] = {stride};
+  const cuuint32_t box[2] = {128, box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void *>(base), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "cuTensorMapEncodeTiled failed (%d) for %llu x %llu, stride %llu, box rows %u", (int)r,
+             (unsigned long long)outer, (unsigned long long)inner, (unsigned long long)stride, box_rows);
+    set_error(buf);
+    return false;
+  }
+  return true;
+}
+
+size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// ------------------------------------------------------------------------------------------- engine
+struct Engine {
+  int dev = -1;
+  cudaStream_t st = nullptr;
+  size_t rows = 0, cols = 0, n = 0, tg = 0, outputs = 0, count = 0, part_len = 0, row1_off = 0, want = 0;
+  size_t resp_len = 0, slot_stride = 0;
+  uint64_t q1 = 0;
+  int q1_bits = 0, threads = 1;
+  bool tail_ok = false;
+  // resident state
+  uint8_t *d_db = nullptr, *d_ub = nullptr, *d_prefix = nullptr;
+  uint32_t *d_that = nullptr, *d_tw = nullptr, *d_err = nullptr;
+  // per-batch scratch, grown on demand
+  size_t cap = 0;
+  uint8_t *d_req = nullptr, *d_qlimb = nullptr, *d_ylimb = nullptr, *d_resp = nullptr;
+  int *d_status = nullptr;
+  uint32_t *d_acc = nullptr, *d_beta = nullptr;
+  int *h_status = nullptr;
+  uint32_t *h_err = nullptr;
+  cudaEvent_t ev[6] = {};
+  CUtensorMap map_db, map_ub;
+  int last_launches = 0;
+};
+
+void free_scratch(Engine *e) {
+  cudaFree(e->d_req);
+  cudaFree(e->d_qlimb);
+  cudaFree(e->d_ylimb);
+  cudaFree(e->d_resp);
+  cudaFree(e->d_status);
+  cudaFree(e->d_acc);
+  cudaFree(e->d_beta);
+  cudaFreeHost(e->h_status);
+  e->d_req = e->d_qlimb = e->d_ylimb = e->d_resp = nullptr;
+  e->d_status = nullptr;
+  e->d_acc = e->d_beta = nullptr;
+  e->h_status = nullptr;
+  e->cap = 0;
+}
+
+void destroy(Engine *e) {
+  if (!e) return;
+  if (e->dev >= 0) cudaSetDevice(e->dev);
+  if (e->st) cudaStreamSynchronize(e->st);
+  free_scratch(e);
+  cudaFree(e->d_db);
+  cudaFree(e->d_ub);
+  cudaFree(e->d_prefix);
+  cudaFree(e->d_that);
+  cudaFree(e->d_tw);
+  cudaFree(e->d_err);
+  cudaFreeHost(e->h_err);
+  for (cudaEvent_t &ev : e->ev)
+    if (ev) cudaEventDestroy(ev);
+  if (e->st) cudaStreamDestroy(e->st);
+  delete e;
+}
+
+bool ensure_capacity(Engine *e, size_t slots) {
+  if (slots <= e->cap) return true;
+  ALTO_CK(cudaStreamSynchronize(e->st));
+  free_scratch(e);
+  const size_t cap = round_up(slots, 4);
+  ALTO_CK(cudaMalloc(&e->d_req, cap * e->slot_stride));
+  ALTO_CK(cudaMalloc(&e->d_qlimb, 4 * cap * e->rows));
+  ALTO_CK(cudaMalloc(&e->d_ylimb, 4 * cap * e->count));
+  ALTO_CK(cudaMalloc(&e->d_resp, cap * e->resp_len));
+  ALTO_CK(cudaMalloc(&e->d_status, cap * sizeof(int)));
+  ALTO_CK(cudaMalloc(&e->d_acc, cap * e->cols * sizeof(uint32_t)));
+  ALTO_CK(cudaMalloc(&e->d_beta, cap * e->cols * sizeof(uint32_t)));
+  ALTO_CK(cudaHostAlloc(&e->h_status, cap * sizeof(int), cudaHostAllocDefault));
+  e->cap = cap;
+  return true;
+}
+
+// ------------------------------------------------------------------------------------------- launch helpers
+template <int BN, alto::Epi EPI>
+bool launch_gemm(const CUtensorMap &a, const CUtensorMap &b, const alto::GemmArgs &g, int units, cudaStream_t st) {
+  const int smem = alto::GemmShape<BN>::kSmemBytes;
+  ALTO_CK(cudaFuncSetAttribute(alto::limb_gemm_kernel<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  alto::limb_gemm_kernel<BN, EPI><<<units, alto::kGemmThreads, smem, st>>>(a, b, g);
+  ALTO_CK(cudaGetLastError());
+  return true;
+}
+
+template <alto::Epi EPI>
+bool dispatch_gemm(int bn, const CUtensorMap &a, const CUtensorMap &b, const alto::GemmArgs &g, int units,
+                   cudaStream_t st) {
+  switch (bn) {
+    case 16: return launch_gemm<16, EPI>(a, b, g, units, st);
+    case 32: return launch_gemm<32, EPI>(a, b, g, units, st);
+    case 64: return launch_gemm<64, EPI>(a, b, g, units, st);
+    case 128: return launch_gemm<128, EPI>(a, b, g, units, st);
+    case 256: return launch_gemm<256, EPI>(a, b, g, units, st);
+  }
+  set_error("unsupported GEMM tile width");
+  return false;
+}
+
+int pick_bn(size_t limb_cols) {
+  for (int bn : {16, 32, 64, 128})
+    if (limb_cols <= (size_t)bn) return bn;
+  return 256;
+}
+
+struct Plan {
+  int bn = 16, num_n = 1;
+  int scan_m = 0, scan_split = 1, scan_kb_per = 1, scan_kb = 0;
+  int pack_m = 0, pack_kb = 0;
+};
+
+Plan make_plan(const Engine *e, size_t slots) {
+  Plan p;
+  const size_t limb_cols = 4 * round_up(slots, 4);
+  p.bn = pick_bn(limb_cols);
+  p.num_n = (int)((limb_cols + p.bn - 1) / p.bn);
+  p.scan_m = (int)((e->cols + alto::kBM - 1) / alto::kBM);
+  p.scan_kb = (int)((e->rows + alto::kBK - 1) / alto::kBK);
+  // Split the record axis so that (a) no chunk exceeds 256 blocks = 32768 records, which bounds every int32 limb
+  // partial sum by 32768 * 255 * 255 < 2^31, and (b) there are about four units per SM, each at least 8 blocks long.
+  const long tiles = (long)p.scan_m * p.num_n;
+  long split = std::max<long>((p.scan_kb + 255) / 256, (4L * 148 + tiles - 1) / tiles);
+  split = std::min<long>(split, std::max<long>(1, p.scan_kb / 8));
+  split = std::max<long>(split, (p.scan_kb + 255) / 256);
+  p.scan_kb_per = (int)((p.scan_kb + split - 1) / split);
+  p.scan_split = (p.scan_kb + p.scan_kb_per - 1) / p.scan_kb_per;
+  p.pack_m = (int)((4 * e->cols + alto::kBM - 1) / alto::kBM);
+  p.pack_kb = (int)(e->count / alto::kBK);
+  return p;
+}
+
+// Enqueues validate .. tail for `slots` staged frames whose statuses go to d_status.  resp/resp_stride receive the
+// response parts of valid frames.
+bool enqueue_batch(Engine *e, const uint8_t *d_slots, size_t slot_stride, size_t slots, uint8_t *resp,
+                   size_t resp_stride, bool host_status) {
+  cudaStream_t st = e->st;
+  const Plan p = make_plan(e, slots);
+  const int bp = (int)round_up(slots, 4);
+  int launches = 0;
+
+  alto::validate_kernel<<<(unsigned)slots, 256, 0, st>>>(d_slots, slot_stride, kSlotLead, e->count, e->rows,
+                                                         e->d_status);
+  ++launches;
+  ALTO_CK(cudaGetLastError());
+  if (host_status) ALTO_CK(cudaMemcpyAsync(e->h_status, e->d_status, slots * sizeof(int), cudaMemcpyDeviceToHost, st));
+  ALTO_CK(cudaEventRecord(e->ev[1], st));
+
+  const unsigned split_threads = 256;
+  {
+    const size_t work = (e->rows / 16) * (size_t)bp;
+    alto::limb_split_kernel<<<(unsigned)((work + split_threads - 1) / split_threads), split_threads, 0, st>>>(
+        d_slots, slot_stride, kSlotLead + 9 + 8 * e->count, (int)slots, bp, e->rows, e->d_qlimb);
+    ++launches;
+    ALTO_CK(cudaGetLastError());
+  }
+  ALTO_CK(cudaMemsetAsync(e->d_acc, 0, slots * e->cols * sizeof(uint32_t), st));
+  CUtensorMap map_q, map_y;
+  if (!make_map(&map_q, e->d_qlimb, e->rows, 4 * (uint64_t)bp, e->rows, (uint32_t)p.bn)) return false;
+  if (!make_map(&map_y, e->d_ylimb, e->count, 4 * (uint64_t)bp, e->count, (uint32_t)p.bn)) return false;
+  {
+    alto::GemmArgs g;
+    g.num_m = p.scan_m;
+    g.num_n = p.num_n;
+    g.kb_total = p.scan_kb;
+    g.kb_per_unit = p.scan_kb_per;
+    g.rows_a = (int)e->cols;
+    g.clients = (int)slots;
+    g.cols = (int)e->cols;
+    g.out = e->d_acc;
+    g.err = e->d_err;
+    if (!dispatch_gemm<alto::Epi::kScan>(p.bn, e->map_db, map_q, g, p.scan_m * p.num_n * p.scan_split, st))
+      return false;
+    ++launches;
+  }
+  ALTO_CK(cudaEventRecord(e->ev[2], st));
+  {
+    const size_t work = (e->count / 16) * (size_t)bp;
+    alto::limb_split_kernel<<<(unsigned)((work + split_threads - 1) / split_threads), split_threads, 0, st>>>(
+        d_slots, slot_stride, kSlotLead + 9, (int)slots, bp, e->count, e->d_ylimb);
+    ++launches;
+    ALTO_CK(cudaGetLastError());
+  }
+  {
+    alto::GemmArgs g;
+    g.num_m = p.pack_m;
+    g.num_n = p.num_n;
+    g.kb_total = p.pack_kb;
+    g.kb_per_unit = p.pack_kb;
+    g.rows_a = (int)(4 * e->cols);
+    g.clients = (int)slots;
+    g.cols = (int)e->cols;
+    g.out = e->d_beta;
+    g.err = e->d_err;
+    if (!dispatch_gemm<alto::Epi::kPack>(p.bn, e->map_ub, map_y, g, p.pack_m * p.num_n, st)) return false;
+    ++launches;
+  }
+  ALTO_CK(cudaEventRecord(e->ev[3], st));
+  {
+    alto::TailArgs t;
+    t.acc = e->d_acc;
+    t.beta = e->d_beta;
+    t.status = e->d_status;
+    t.req = d_slots;
+    t.req_stride = slot_stride;
+    t.z_off = kSlotLead + 9 + 4 * e->count;
+    t.that = e->d_that;
+    t.twiddle = e->d_tw;
+    t.prefix = e->d_prefix;
+    t.resp = resp;
+    t.resp_stride = resp_stride;
+    t.n = (int)e->n;
+    t.tg = (int)e->tg;
+    t.outputs = (int)e->outputs;
+    t.cols = (int)e->cols;
+    t.part_len = (int)e->part_len;
+    t.row1_off = (int)e->row1_off;
+    t.q1_bits = e->q1_bits;
+    t.q1 = (int64_t)e->q1;
+    const size_t smem = (e->n + (e->part_len + 3) / 4 + 1) * sizeof(uint32_t);
+    if (smem > 48 * 1024) ALTO_CK(cudaFuncSetAttribute(alto::tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    alto::tail_kernel<<<(unsigned)(slots * e->outputs), 256, smem, st>>>(t);
+    ++launches;
+    ALTO_CK(cudaGetLastError());
+  }
+  ALTO_CK(cudaEventRecord(e->ev[4], st));
+  e->last_launches = launches;
+  return true;
+}
+
+// Groups consecutive items whose source and destination addresses advance by constant pitches into one 2-D copy.
+template <class SrcAt, class DstAt>
+bool copy_runs(size_t items, size_t width, SrcAt src_at, DstAt dst_at, cudaMemcpyKind kind, cudaStream_t st) {
+  size_t i = 0;
+  while (i < items) {
+    size_t j = i + 1;
+    long long sp = 0, dp = 0;
+    if (j < items) {
+      sp = (long long)((const char *)src_at(j) - (const char *)src_at(i));
+      dp = (long long)((const char *)dst_at(j) - (const char *)dst_at(i));
+      if (sp >= (long long)width && dp >= (long long)width) {
+        while (j + 1 < items && (const char *)src_at(j + 1) - (const char *)src_at(j) == sp &&
+               (const char *)dst_at(j + 1) - (const char *)dst_at(j) == dp)
+          ++j;
+        ++j;
+      } else {
+        j = i + 1;
+      }
+    }
+    if (j - i == 1) {
+      ALTO_CK(cudaMemcpyAsync(dst_at(i), src_at(i), width, kind, st));
+    } else {
+      ALTO_CK(cudaMemcpy2DAsync(dst_at(i), (size_t)dp, src_at(i), (size_t)sp, width, j - i, kind, st));
+    }
+    i = j;
+  }
+  return true;
+}
+
+bool finish(Engine *e, double *stage_ms, int launches_extra) {
+  (void)launches_extra;
+  ALTO_CK(cudaMemcpyAsync(e->h_err, e->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->st));
+  ALTO_CK(cudaStreamSynchronize(e->st));
+  if (*e->h_err) {
+    char buf[96];
+    snprintf(buf, sizeof buf, "a kernel wait timed out (device error word 0x%x)", *e->h_err);
+    set_error(buf);
+    return false;
+  }
+  if (stage_ms) {
+    float t[5];
+    for (int i = 0; i < 5; ++i) ALTO_CK(cudaEventElapsedTime(&t[i], e->ev[0], e->ev[i + 1]));
+    stage_ms[0] = t[0];
+    stage_ms[1] = t[1] - t[0];
+    stage_ms[2] = t[2] - t[1];
+    stage_ms[3] = t[4] - t[2];
+  }
+  return true;
+}
+
+bool host_header_status(const Engine *e, const uint8_t *f, size_t len, int *status) {
+  if (!f || len != e->want) {
+    *status = 1;
+    return false;
+  }
+  uint32_t c1, c2;
+  memcpy(&c1, f + 1, 4);
+  memcpy(&c2, f + 5, 4);
+  if (f[0] != 0 || c1 != e->count || c2 != e->count) {
+    *status = 2;
+    return false;
+  }
+  return true;
+}
+
+int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t b, uint8_t *const *out, int *status,
+                double *stage_ms) {
+  std::vector<size_t> cand;
+  cand.reserve(b);
+  for (size_t c = 0; c < b; ++c)
+    if (host_header_status(e, req[c], len[c], &status[c])) cand.push_back(c);
+  if (stage_ms) std::fill(stage_ms, stage_ms + 4, 0.0);
+  e->last_launches = 0;
+  if (cand.empty()) return 0;
+  if (!e->tail_ok) {
+    // The reference computes the statuses, then fails in the tail (src/amx_kernels.cpp:610).
+    for (size_t c : cand) {
+      int bad = 0;
+      for (size_t i = 0; i < 2 * e->count; ++i) {
+        uint32_t v;
+        memcpy(&v, req[c] + 9 + 4 * i, 4);
+        bad |= v >= (uint32_t)alto::kQ;
+      }
+      status[c] = bad ? 3 : 0;
+    }
+    return -3;
+  }
+  if (cudaSetDevice(e->dev) != cudaSuccess || !ensure_capacity(e, cand.size())) return -4;
+  cudaStream_t st = e->st;
+  if (cudaMemsetAsync(e->d_err, 0, sizeof(uint32_t), st) != cudaSuccess) return -4;
+  if (cudaEventRecord(e->ev[0], st) != cudaSuccess) return -4;
+  if (!copy_runs(
+          cand.size(), e->want, [&](size_t i) { return (const void *)req[cand[i]]; },
+          [&](size_t i) { return (void *)(e->d_req + i * e->slot_stride + kSlotLead); }, cudaMemcpyHostToDevice, st))
+    return -4;
+  if (!enqueue_batch(e, e->d_req, e->slot_stride, cand.size(), e->d_resp, e->resp_len, true)) return -4;
+  if (cudaEventSynchronize(e->ev[1]) != cudaSuccess) {
+    set_error("status event failed");
+    return -4;
+  }
+  std::vector<size_t> ok;  // indices into cand with status 0
+  for (size_t i = 0; i < cand.size(); ++i) {
+    status[cand[i]] = e->h_status[i];
+    if (e->h_status[i] == 0) ok.push_back(i);
+  }
+  if (!copy_runs(
+          ok.size(), e->resp_len, [&](size_t k) { return (const void *)(e->d_resp + ok[k] * e->resp_len); },
+          [&](size_t k) { return (void *)out[cand[ok[k]]]; }, cudaMemcpyDeviceToHost, st))
+    return -4;
+  if (cudaEventRecord(e->ev[5], st) != cudaSuccess) return -4;
+  if (!finish(e, stage_ms, 0)) return -4;
+  return (int)ok.size();
+}
+
+}  // namespace
+
+// ============================================================================================ C ABI
+extern "C" {
+
+const char *alto_last_error(void) { return g_last_error.c_str(); }
+
+int sw_amx_init(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    set_error("no CUDA device");
+    return -1;
+  }
+  if (cudaFree(nullptr) != cudaSuccess) {
+    set_error("cannot create a CUDA context");
+    return -1;
+  }
+  return 0;
+}
+
+void *alto_engine_new(const uint8_t *db_col, const uint8_t *db_tiled, size_t ld, size_t rows, size_t cols,
+                      const int8_t *ub, size_t n, size_t tg, const uint8_t *const *prefix, size_t part_len,
+                      size_t row1_off, uint64_t q1, int q1_bits, const uint64_t *const *that,
+                      const uint64_t *inv_table, uint64_t q, int threads) {
+  // The reference's checks (src/amx_kernels.cpp:551-552), then this engine's own limits.
+  if (!db_col || !db_tiled || !ub || !prefix || !that || !inv_table || q != alto::kQ || !n || n > 4096 || n % 16 ||
+      cols % n || rows % 64 || cols % 32 || threads <= 0 || (tg * n) % 128) {
+    set_error("unsupported engine configuration");
+    return nullptr;
+  }
+  if (tg < 1 || tg * n > 32768 || ld < rows || !rows || !cols) {
+    set_error("configuration outside this engine's limits (1 <= tg, tg * n <= 32768, ld >= rows > 0)");
+    return nullptr;
+  }
+  Engine *e = new Engine;
+  e->rows = rows;
+  e->cols = cols;
+  e->n = n;
+  e->tg = tg;
+  e->outputs = cols / n;
+  e->count = tg * n;
+  e->part_len = part_len;
+  e->row1_off = row1_off;
+  e->q1 = q1;
+  e->q1_bits = q1_bits;
+  e->threads = threads;
+  e->want = 9 + 4 * (2 * e->count + rows);
+  e->resp_len = e->outputs * part_len;
+  e->slot_stride = round_up(kSlotLead + e->want, 256);
+  // The reference's tail checks (src/amx_kernels.cpp:463, 517), evaluated once here and reported per batch.
+  e->tail_ok = n >= 16 && (n & (n - 1)) == 0 && q1 < (1ull << 21) && n % 8 == 0 &&
+               (row1_off + n * (size_t)q1_bits + 7) / 8 <= part_len && q1_bits <= 24;
+  auto fail = [&](const char *where, cudaError_t err) -> void * {
+    set_error(where, err);
+    destroy(e);
+    return nullptr;
+  };
+  cudaError_t err;
+  if ((err = cudaGetDevice(&e->dev)) != cudaSuccess) return fail("cudaGetDevice", err);
+  if ((err = cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking)) != cudaSuccess) return fail("stream", err);
+  for (cudaEvent_t &ev : e->ev)
+    if ((err = cudaEventCreate(&ev)) != cudaSuccess) return fail("event", err);
+  if ((err = cudaMalloc(&e->d_db, rows * cols)) != cudaSuccess) return fail("database", err);
+  if ((err = cudaMemcpy2D(e->d_db, rows, db_col, ld, rows, cols, cudaMemcpyHostToDevice)) != cudaSuccess)
+    return fail("database upload", err);
+  if ((err = cudaMalloc(&e->d_ub, 4 * e->count * cols)) != cudaSuccess) return fail("packing matrix", err);
+  if ((err = cudaMemcpy(e->d_ub, ub, 4 * e->count * cols, cudaMemcpyHostToDevice)) != cudaSuccess)
+    return fail("packing matrix upload", err);
+  {
+    std::vector<uint32_t> th(e->outputs * e->count);
+    for (size_t o = 0; o < e->outputs; ++o)
+      for (size_t k = 0; k < e->count; ++k) th[o * e->count + k] = (uint32_t)(that[o][k] % alto::kQ);
+    if ((err = cudaMalloc(&e->d_that, th.size() * 4)) != cudaSuccess) return fail("bold_t_hat", err);
+    if ((err = cudaMemcpy(e->d_that, th.data(), th.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess)
+      return fail("bold_t_hat upload", err);
+    std::vector<uint32_t> tw(n);
+    for (size_t i = 0; i < n; ++i) tw[i] = (uint32_t)(inv_table[i] & 0xffffffffu);
+    if ((err = cudaMalloc(&e->d_tw, n * 4)) != cudaSuccess) return fail("inverse table", err);
+    if ((err = cudaMemcpy(e->d_tw, tw.data(), n * 4, cudaMemcpyHostToDevice)) != cudaSuccess)
+      return fail("inverse table upload", err);
+    std::vector<uint8_t> pre(e->outputs * part_len);
+    for (size_t o = 0; o < e->outputs; ++o) memcpy(pre.data() + o * part_len, prefix[o], part_len);
+    if ((err = cudaMalloc(&e->d_prefix, pre.size() ? pre.size() : 1)) != cudaSuccess) return fail("prefixes", err);
+    if (!pre.empty() && (err = cudaMemcpy(e->d_prefix, pre.data(), pre.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+      return fail("prefix upload", err);
+  }
+  if ((err = cudaMalloc(&e->d_err, sizeof(uint32_t))) != cudaSuccess) return fail("error word", err);
+  if ((err = cudaMemset(e->d_err, 0, sizeof(uint32_t))) != cudaSuccess) return fail("error word", err);
+  if ((err = cudaHostAlloc(&e->h_err, sizeof(uint32_t), cudaHostAllocDefault)) != cudaSuccess)
+    return fail("pinned error word", err);
+  if (!make_map(&e->map_db, e->d_db, rows, cols, rows, alto::kBM) ||
+      !make_map(&e->map_ub, e->d_ub, e->count, 4 * cols, e->count, alto::kBM)) {
+    destroy(e);
+    return nullptr;
+  }
+  return e;
+}
+
+void alto_engine_free(void *p) { destroy(static_cast<Engine *>(p)); }
+
+size_t alto_request_len(const void *p) {
+  const Engine *e = static_cast<const Engine *>(p);
+  return 9 + 4 * (2 * e->tg * e->n + e->rows);
+}
+
+size_t alto_response_len(const void *p) {
+  const Engine *e = static_cast<const Engine *>(p);
+  return e->outputs * e->part_len;
+}
+
+int alto_answer(void *p, const uint8_t *const *req, const size_t *len, size_t b, uint8_t *const *out, int *status,
+                int method, double *stage_ms) {
+  Engine *e = static_cast<Engine *>(p);
+  if (!e || !req || !len || !out || !status || (method != 0 && method != 2)) return -1;
+  return answer_host(e, req, len, b, out, status, stage_ms);
+}
+
+int alto_answer_device(void *p, const uint8_t *d_req, size_t req_stride, size_t b, uint8_t *d_out, size_t out_stride,
+                       int *status, double *stage_ms) {
+  Engine *e = static_cast<Engine *>(p);
+  if (!e || !d_req || !d_out || !status || req_stride % 16 || req_stride < round_up(kSlotLead + e->want, 16) ||
+      out_stride < e->resp_len)
+    return -1;
+  if (stage_ms) std::fill(stage_ms, stage_ms + 4, 0.0);
+  e->last_launches = 0;
+  if (!b) return 0;
+  if (!e->tail_ok) return -3;
+  if (cudaSetDevice(e->dev) != cudaSuccess || !ensure_capacity(e, b)) return -4;
+  if (cudaMemsetAsync(e->d_err, 0, sizeof(uint32_t), e->st) != cudaSuccess) return -4;
+  if (cudaEventRecord(e->ev[0], e->st) != cudaSuccess) return -4;
+  if (!enqueue_batch(e, d_req, req_stride, b, d_out, out_stride, true)) return -4;
+  if (cudaEventRecord(e->ev[5], e->st) != cudaSuccess) return -4;
+  if (!finish(e, stage_ms, 0)) return -4;
+  int valid = 0;
+  for (size_t c = 0; c < b; ++c) {
+    status[c] = e->h_status[c];
+    valid += status[c] == 0;
+  }
+  return valid;
+}
+
+int alto_last_launches(const void *p) { return p ? static_cast<const Engine *>(p)->last_launches : 0; }
+
+int alto_synthetic_db_col_device(uint8_t *d_db, size_t ld, size_t rows, size_t col0, size_t ncols) {
+  if (rows % 4 || ld % 4) return -1;
+  const size_t work = (rows / 4) * ncols;
+  alto::synthetic_db_kernel<<<(unsigned)((work + 255) / 256), 256>>>(d_db, ld, rows, col0, ncols);
+  const cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    set_error("synthetic database", e);
+    return -1;
+  }
+  return 0;
+}
+
+}  // extern "C"

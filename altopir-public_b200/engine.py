@@ -1,0 +1,135 @@
+"""Engine wrapper mirroring the reference's Rust binding (src/engine.rs): Method, MappedBytes-style host buffers,
+TiledDb, build_packing_matrix and Engine, all calling the C ABI of libaltopir_gpu.so."""
+import ctypes
+import enum
+
+import numpy as np
+
+from . import lib, last_error
+from .service import Q
+
+
+class Method(enum.IntEnum):
+    """Engine.rs Method codes (src/engine.rs:22-50).  The GPU engine accepts both and runs the same path."""
+    AMX = 0
+    VNNI = 2
+
+
+def init():
+    """engine::init_amx (src/engine.rs:66-69): here, create the CUDA context; raises without a usable device."""
+    r = lib().sw_amx_init()
+    if r != 0:
+        raise RuntimeError(f"no usable CUDA device: {last_error()}")
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _ptrs(arrays):
+    return (ctypes.c_void_p * len(arrays))(*[a.ctypes.data for a in arrays])
+
+
+class TiledDb:
+    """TiledDb::new (src/engine.rs:111-118): sw_tile_db into a buffer of rows * cols bytes."""
+
+    def __init__(self, db_col, ld, rows, cols, threads=1):
+        assert rows % 64 == 0 and cols % 32 == 0 and db_col.size >= (cols - 1) * ld + rows
+        self.rows, self.cols = rows, cols
+        self.buf = np.empty(rows * cols, dtype=np.uint8)
+        lib().sw_tile_db(_p(self.buf), _p(db_col), ld, rows, cols, threads)
+
+
+def build_packing_matrix(ub, bold_t, bold_t_bar, tables, gen_pows, num_iter, tg, n, qmod=Q, threads=1):
+    """build_packing_matrix (src/engine.rs:127-138) over sw_pack_build."""
+    rho = len(bold_t)
+    assert ub.size == 4 * tg * n * rho * n and len(bold_t_bar) == rho
+    assert tables.size == n * n and gen_pows.size >= num_iter
+    for s in list(bold_t) + list(bold_t_bar):
+        assert s.size >= num_iter * tg * n and s.dtype == np.uint64
+    tables = np.ascontiguousarray(tables, dtype=np.uint32)     # held here: ctypes keeps only the address
+    gen_pows = np.ascontiguousarray(gen_pows, dtype=np.uint32)
+    lib().sw_pack_build(_p(ub), _ptrs(bold_t), _ptrs(bold_t_bar), _p(tables), _p(gen_pows), num_iter, tg, n, rho,
+                        qmod, threads)
+
+
+class EngineError(RuntimeError):
+    pass
+
+
+class Engine:
+    """Engine<'a> (src/engine.rs:140-195).  The device copies every input at construction, so the arrays passed
+    here may be dropped afterwards."""
+
+    def __init__(self, db_col, tiled, ld, ub, n, tg, prefixes, row1_off, q1, q1_bits, that, inv_table, q=Q,
+                 threads=1):
+        rows, cols = tiled.rows, tiled.cols
+        assert db_col.size >= (cols - 1) * ld + rows and ub.size == 4 * tg * n * cols and len(prefixes) == cols // n
+        assert len(that) == cols // n and all(t.size >= tg * n for t in that) and inv_table.size >= n
+        part_len = prefixes[0].size
+        assert all(p.size == part_len for p in prefixes)
+        # arrays converted here are held in locals until the call returns: ctypes keeps only their addresses
+        pre = [np.ascontiguousarray(p, dtype=np.uint8) for p in prefixes]
+        that64 = [np.ascontiguousarray(t, dtype=np.uint64) for t in that]
+        inv = np.ascontiguousarray(inv_table, dtype=np.uint64)
+        db_col = np.ascontiguousarray(db_col)
+        ub = np.ascontiguousarray(ub)
+        self.ptr = lib().alto_engine_new(_p(db_col), _p(tiled.buf), ld, rows, cols, _p(ub), n, tg, _ptrs(pre),
+                                         part_len, row1_off, q1, q1_bits, _ptrs(that64), _p(inv), q, threads)
+        if not self.ptr:
+            raise EngineError(f"unsupported engine configuration: {last_error()}")
+
+    @staticmethod
+    def from_state(st, threads=1):
+        """Prepared::engine (src/service.rs:159-170) for a service.SyntheticState."""
+        p = st.p
+        tiled = TiledDb(st.db_col, st.db_col.shape[1], p.rows, p.record_bytes, threads)
+        return Engine(st.db_col, tiled, st.db_col.shape[1], st.ub, p.n, p.tg, st.prefixes, p.row1_off, 1 << p.q1_bits,
+                      p.q1_bits, st.that, st.inv_table, Q, threads)
+
+    def request_len(self):
+        return lib().alto_request_len(self.ptr)
+
+    def response_len(self):
+        return lib().alto_response_len(self.ptr)
+
+    def answer(self, reqs, out, status, method=Method.AMX):
+        """Engine::answer (src/engine.rs:174-188).  reqs: a sequence of uint8 arrays (or a 2-D array, one frame per
+        row); out: a (b, response_len) uint8 array or a sequence of uint8 arrays; status: int32 array of b.
+        Returns (answered, stage_ms[4]); raises EngineError on a negative return."""
+        b = len(reqs)
+        frames = [reqs[i] for i in range(b)]
+        outs = [out[i] for i in range(b)]
+        assert len(outs) == b and status.size == b and status.dtype == np.int32
+        rl = self.response_len()
+        assert all(o.size == rl and o.dtype == np.uint8 and o.flags.c_contiguous for o in outs)
+        req_p = (ctypes.c_void_p * b)(*[f.ctypes.data if f is not None else None for f in frames])
+        lens = (ctypes.c_size_t * b)(*[f.size if f is not None else 0 for f in frames])
+        out_p = (ctypes.c_void_p * b)(*[o.ctypes.data for o in outs])
+        stage = (ctypes.c_double * 4)()
+        r = lib().alto_answer(self.ptr, req_p, lens, b, out_p,
+                              status.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), int(method), stage)
+        if r < 0:
+            raise EngineError(f"engine error {r}: {last_error()}")
+        return r, list(stage)
+
+    def answer_raw(self, req_ptrs, lens, b, out_ptrs, status, method=Method.AMX, stage=None):
+        """alto_answer on prepared ctypes arrays (no per-call Python list building); returns the raw code."""
+        return lib().alto_answer(self.ptr, req_ptrs, lens, b, out_ptrs,
+                                 status.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), int(method), stage)
+
+    def answer_device(self, d_req, req_stride, b, d_out, out_stride, status, stage=None):
+        """alto_answer_device: frames already in device memory (frame c at d_req + c * req_stride + 7)."""
+        return lib().alto_answer_device(self.ptr, ctypes.c_void_p(d_req), req_stride, b, ctypes.c_void_p(d_out),
+                                        out_stride, status.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), stage)
+
+    def last_launches(self):
+        return lib().alto_last_launches(self.ptr)
+
+    def close(self):
+        if getattr(self, "ptr", None):
+            lib().alto_engine_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        self.close()

@@ -1,0 +1,122 @@
+/*
+ * altopir_gpu.h -- C ABI of the B200 AltoPIR answer engine (libaltopir_gpu.so).
+ *
+ * The first block is a drop-in for the reference engine's C ABI: the same symbols, signatures, argument meaning,
+ * return codes and ownership rules that the reference's Rust wrapper binds (src/engine.rs:4-20), so a build that
+ * links this library instead of compiling src/amx_kernels.cpp needs no change to the Rust side.  The answer path
+ * runs on the current CUDA device (one engine per device); there is no CPU fallback: without a usable GPU,
+ * sw_amx_init() and alto_engine_new() fail.
+ *
+ * The second block holds extensions with no counterpart in the reference.
+ */
+#ifndef ALTOPIR_GPU_H
+#define ALTOPIR_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ================================================================ reference C ABI (src/engine.rs:4-20) */
+
+/* Replaces sw_amx_init (src/amx_kernels.cpp:151), which asks the kernel for AMX tile state.  Here it creates the
+ * CUDA context on the current device.  Returns 0 on success, -1 when no usable CUDA device is present. */
+int sw_amx_init(void);
+
+/* Replace sw_alloc_zeroed / sw_alloc / sw_free (src/amx_kernels.cpp:97-113): anonymous host mappings aligned to
+ * 2 MiB (zero-filled for sw_alloc_zeroed); sw_free(NULL) is a no-op.  Used by the caller for the tiled database and
+ * the packing matrix, which alto_engine_new copies into device memory. */
+void *sw_alloc_zeroed(size_t bytes);
+void *sw_alloc(size_t bytes);
+void sw_free(void *p);
+
+/* Replaces sw_tile_db (src/amx_kernels.cpp:138-149).  Copies the k x m column-order database db[col * ld + r]
+ * into dst as a compact column-order matrix dst[col * k + r] (k records per column, no padding).  This is the
+ * engine's own tiled layout: the device reads it in 128-record x 128-column boxes through TMA, so no further
+ * host-side tiling exists.  Uses `threads` host threads. */
+void sw_tile_db(uint8_t *dst, const uint8_t *db, size_t ld, size_t k, size_t m, int threads);
+
+/* Replaces sw_pack_build (src/amx_kernels.cpp:311-341).  Folds the InspiRING automorphisms into the dense packing
+ * matrix U ((rho * n) columns x (tg * n) key words, values mod q) exactly as the reference does and stores it in
+ * this engine's layout: ub[(col * 4 + j) * (tg * n) + k] = byte j of U[col][k] (4 * tg * n * rho * n bytes, the
+ * same size as the reference's buffer).  q must be 4294955009. */
+void sw_pack_build(int8_t *ub, const uint64_t *const *bold_t, const uint64_t *const *bold_t_bar,
+                   const uint32_t *tables, const uint32_t *gen_pows, size_t num_iter, size_t tg, size_t n, size_t rho,
+                   uint64_t q, int threads);
+
+/* Replaces alto_engine_new (src/amx_kernels.cpp:546-560).  Same configuration checks as the reference (NULL for
+ * q != 4294955009, n == 0, n > 4096, n % 16, cols % n, rows % 64, cols % 32, threads <= 0, (tg * n) % 128, or a
+ * NULL pointer), plus two limits of this engine: 1 <= tg and tg * n <= 32768 (keeps every int32 limb partial sum
+ * of the packing product exact).  The database is read from db_col (db_col[col * ld + r], r < rows, col < cols);
+ * db_tiled must be non-NULL but is not read.  The database, the packing matrix `ub` (layout of sw_pack_build),
+ * the row-0 prefixes (cols / n buffers of part_len bytes), bold_t_hat (`that`, cols / n arrays of tg * n words,
+ * reduced mod q) and the low 32 bits of inv_table[0..n) are copied into device memory, so the caller may free all
+ * of them once this returns.  Returns NULL when the configuration is unsupported or the device lacks memory
+ * (alto_last_error() says which). */
+void *alto_engine_new(const uint8_t *db_col, const uint8_t *db_tiled, size_t ld, size_t rows, size_t cols,
+                      const int8_t *ub, size_t n, size_t tg, const uint8_t *const *prefix, size_t part_len,
+                      size_t row1_off, uint64_t q1, int q1_bits, const uint64_t *const *that,
+                      const uint64_t *inv_table, uint64_t q, int threads);
+
+/* Replaces alto_engine_free (src/amx_kernels.cpp:561).  NULL is a no-op. */
+void alto_engine_free(void *engine);
+
+/* Replace alto_request_len / alto_response_len (src/amx_kernels.cpp:562-563):
+ * 9 + 4 * (2 * tg * n + rows) and (cols / n) * part_len. */
+size_t alto_request_len(const void *engine);
+size_t alto_response_len(const void *engine);
+
+/* Replaces alto_answer (src/amx_kernels.cpp:564-615).  Answers a batch of b request frames in host memory:
+ *   status[c] = 1 for a NULL frame or a length other than alto_request_len, 2 for a flag byte != 0 or a key count
+ *   != tg * n, 3 for a y or z key word >= q, else 0 (query words are not range-checked);
+ *   out[c] (alto_response_len bytes) is written for status 0 only, other output buffers stay untouched.
+ * method must be 0 (the reference's AMX code) or 2 (VNNI); both run the same GPU path.  When stage_ms is not NULL
+ * it receives device times in ms of [0] upload + validation, [1] limb split + scan, [2] pack, [3] tail + download.
+ * Returns the number of valid requests, -1 for bad arguments, -3 when the tail parameters are invalid (n not a
+ * power of two >= 16, q1 >= 2^21, q1_bits > 24, n % 8, or row 1 not fitting in part_len), -4 when the device
+ * failed (CUDA error or a kernel wait that timed out; alto_last_error() has the reason).  Calls on one engine must
+ * not overlap; different engines may be used from different threads.  Pinned host buffers make the copies
+ * asynchronous DMA; pageable buffers work but copy through a staging buffer. */
+int alto_answer(void *engine, const uint8_t *const *req, const size_t *len, size_t b, uint8_t *const *out,
+                int *status, int method, double *stage_ms);
+
+/* ================================================================ extensions (no counterpart in the reference) */
+
+/* Text of the last error recorded by this library on the calling thread ("" if none). */
+const char *alto_last_error(void);
+
+/* alto_answer for frames that are already resident in device memory: frame c starts at d_req + c * req_stride
+ * (full frames including the 9-byte header, req_stride >= alto_request_len and a multiple of 16; the header is
+ * checked on the device), responses go to d_out + c * out_stride (device memory, out_stride >= alto_response_len),
+ * statuses to the host array status[b].  Returns what alto_answer returns. */
+int alto_answer_device(void *engine, const uint8_t *d_req, size_t req_stride, size_t b, uint8_t *d_out,
+                       size_t out_stride, int *status, double *stage_ms);
+
+/* Counts of kernel launches issued by the most recent alto_answer / alto_answer_device call of this engine. */
+int alto_last_launches(const void *engine);
+
+/* Deterministic synthetic inputs (test and benchmark data; not part of the answer path).
+ * alto_synthetic_db_col: db[(col - col0) * ld + r] = byte col of the reference's synthetic record r
+ *   (src/service.rs:43-62, splitmix64 seed 0x416c746f504952), for r < rows and ncols columns from col0.
+ * alto_synthetic_db_col_device: the same into device memory (rows % 4 == 0, ld % 4 == 0); 0 on success.
+ * alto_fill_uniform_u32: dst[i] = a uniform value in [0, bound) drawn from splitmix64 counter `seed` + i.
+ * alto_fill_uniform_u64: the same with 64-bit outputs (bound <= 2^32).
+ * alto_fill_bytes: dst[i] = uniform bytes from the same counter construction.
+ * alto_synthetic_request: a well-formed frame of alto_request_len bytes for a seeded client: y, z uniform in
+ *   [0, 4294955009), query words uniform over u32 (the distribution of rounded RLWE query words).
+ * alto_pack_encode: packing-matrix values U[col * K + k] (< 2^32) into the layout of sw_pack_build. */
+void alto_synthetic_db_col(uint8_t *db, size_t ld, size_t rows, size_t col0, size_t ncols, int threads);
+int alto_synthetic_db_col_device(uint8_t *d_db, size_t ld, size_t rows, size_t col0, size_t ncols);
+void alto_fill_uniform_u32(uint32_t *dst, size_t count, uint64_t bound, uint64_t seed, int threads);
+void alto_fill_uniform_u64(uint64_t *dst, size_t count, uint64_t bound, uint64_t seed, int threads);
+void alto_fill_bytes(uint8_t *dst, size_t count, uint64_t seed, int threads);
+void alto_synthetic_request(uint8_t *frame, size_t rows, size_t tg_n, uint64_t seed, uint64_t client);
+void alto_pack_encode(int8_t *ub, const uint32_t *U, size_t cols, size_t K, int threads);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ALTOPIR_GPU_H */

@@ -1,0 +1,168 @@
+"""Parity of the CUDA engine with the reference, through the C ABI (alto_answer): byte-for-byte against the golden
+vectors the reference engine produced (tests/golden/) and against the oracle restatement on the same seeded
+inputs.  Mirrors the reference's tests/engine.rs (responses, malformed and mutated frames, multi-block and chunked
+batches) and adds the larger configurations of the benchmark."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_DIR, sha
+import frames as fr
+
+pytestmark = pytest.mark.gpu
+
+
+def _engine(svc, eng, rows, rb, seed, full_prefix=False, keep_values=True):
+    p = svc.params(rows, rb)
+    st = svc.SyntheticState.make(p, seed=seed, full_prefix=full_prefix, keep_values=keep_values)
+    return p, st, eng.Engine.from_state(st, threads=svc.threads())
+
+
+def _answer(e, frames, fill=0):
+    b = len(frames)
+    out = np.full((b, e.response_len()), fill, dtype=np.uint8)
+    status = np.full(b, -1, dtype=np.int32)
+    n, stage = e.answer(frames, out, status)
+    return n, status, out
+
+
+def test_small_matches_golden_and_oracle(gpu, golden, oracle, svc, eng):
+    g = golden["cases"]["small"]
+    p, st, e = _engine(svc, eng, g["rows"], g["record_bytes"], g["state_seed"], g["full_prefix"])
+    assert e.request_len() == svc.request_len(p) and e.response_len() == svc.response_len(p)
+    req = svc.synthetic_requests(p, g["b"], seed=g["request_seed"])
+    n, status, out = _answer(e, [req[i] for i in range(g["b"])])
+    assert n == g["b"] and list(status) == g["status"]
+    assert [sha(out[i]) for i in range(g["b"])] == g["sha256"]
+    assert np.array_equal(out[0], np.fromfile(os.path.join(GOLDEN_DIR, "resp_small_0.bin"), dtype=np.uint8))
+    r, ost, oout = oracle.answer(st, [req[i] for i in range(g["b"])])
+    assert np.array_equal(out, oout)
+    for method in (eng.Method.AMX, eng.Method.VNNI):
+        out2 = np.zeros_like(out)
+        status2 = np.full(g["b"], -1, dtype=np.int32)
+        e.answer([req[i] for i in range(g["b"])], out2, status2, method)
+        assert np.array_equal(out2, out)
+    e.close()
+
+
+def test_malformed_requests_are_rejected_like_the_decoder(gpu, golden, svc, eng):
+    p, st, e = _engine(svc, eng, 2048, 4096, 3, True)
+    g = golden["cases"]["malformed"]
+    r0 = svc.synthetic_requests(p, 1, seed=g["request_seed"], first_client=0)[0]
+    r1 = svc.synthetic_requests(p, 1, seed=g["request_seed"], first_client=1)[0]
+    mf, want = fr.malformed_table(r0, r1, p.count)
+    n, status, arena = _answer(e, mf, fill=0xA5)
+    assert n == 2 and list(status) == want
+    for c in range(1, 7):
+        assert (arena[c] == 0xA5).all(), "a rejected buffer was written"
+    assert [sha(arena[0]), sha(arena[7])] == g["sha256_valid"]
+    # a NULL frame is status 1 as well
+    frames_ = [None, r0]
+    n, status, out = _answer(e, frames_, fill=0x5A)
+    assert n == 1 and list(status) == [1, 0] and (out[0] == 0x5A).all()
+    e.close()
+
+
+def test_mutated_frames_agree_with_reference_statuses(gpu, golden, oracle, svc, eng):
+    p, st, e = _engine(svc, eng, 2048, 4096, 3, True)
+    gm = golden["cases"]["mutated"]
+    base = [svc.synthetic_requests(p, 1, seed=gm["request_seed"], first_client=i)[0] for i in range(4)]
+    for batch, want in zip(fr.mutated_batches(base, p.count), gm["status"]):
+        n, status, out = _answer(e, batch, fill=0x33)
+        assert list(status) == want
+        assert n == sum(s == 0 for s in want)
+        for i, s in enumerate(want):
+            if s != 0:
+                assert (out[i] == 0x33).all()
+        ok = [i for i, s in enumerate(want) if s == 0]
+        if ok:
+            r, ost, oout = oracle.answer(st, [batch[i] for i in ok[:4]])
+            assert np.array_equal(out[ok[:4]], oout)
+    e.close()
+
+
+def test_multi_block_and_chunked_batches_match_golden(gpu, golden, svc, eng):
+    g = golden["cases"]["multiblock"]
+    p, st, e = _engine(svc, eng, g["rows"], g["record_bytes"], g["state_seed"])
+    for b, case in g["batches"].items():
+        b = int(b)
+        req = svc.synthetic_requests(p, b, seed=case["request_seed"])
+        n, status, out = _answer(e, [req[i] for i in range(b)])
+        assert n == b and (status == 0).all()
+        assert sha(out) == case["sha256"], f"batch {b}"
+    e.close()
+
+
+def test_plain_small_config_matches_golden(gpu, golden, svc, eng):
+    g = golden["cases"]["plain_2048x32k"]
+    p, st, e = _engine(svc, eng, g["rows"], g["record_bytes"], g["state_seed"])
+    req = svc.synthetic_requests(p, 1, seed=g["request_seed"])
+    n, status, out = _answer(e, [req[0]])
+    assert n == 1 and sha(out) == g["sha256"]
+    e.close()
+
+
+def test_each_response_is_the_same_alone_and_in_the_mix(gpu, oracle, svc, eng):
+    p, st, e = _engine(svc, eng, 4096, 8192, 17, True)
+    req = svc.synthetic_requests(p, 37, seed=18)
+    frames_ = [req[i] for i in range(37)]
+    n, status, mixed = _answer(e, frames_)
+    assert n == 37
+    for i in (0, 5, 36):
+        n1, s1, alone = _answer(e, [frames_[i]])
+        assert n1 == 1 and np.array_equal(alone[0], mixed[i])
+    r, ost, oout = oracle.answer(st, frames_)
+    assert np.array_equal(mixed, oout)
+    # capacity shrinking and growing between calls
+    for b in (3, 37, 1):
+        n, status, out = _answer(e, frames_[:b])
+        assert np.array_equal(out, mixed[:b])
+    e.close()
+
+
+def test_device_resident_path_matches_host_path(gpu, svc, eng):
+    import torch
+    p, st, e = _engine(svc, eng, 2048, 4096, 23)
+    b = 9
+    req = svc.synthetic_requests(p, b, seed=24)
+    n, status, want = _answer(e, [req[i] for i in range(b)])
+    stride = (7 + e.request_len() + 15) // 16 * 16
+    slots = torch.zeros((b, stride), dtype=torch.uint8, device="cuda")
+    slots[:, 7:7 + e.request_len()] = torch.from_numpy(req).cuda()
+    slots[4, 7 + 9] = 0xFF  # key word out of range in frame 4: y[0] >= Q
+    slots[4, 7 + 10:7 + 13] = 0xFF
+    d_out = torch.zeros((b, e.response_len()), dtype=torch.uint8, device="cuda")
+    st_dev = np.full(b, -1, dtype=np.int32)
+    r = e.answer_device(slots.data_ptr(), stride, b, d_out.data_ptr(), e.response_len(), st_dev)
+    torch.cuda.synchronize()
+    assert r == b - 1 and list(st_dev) == [0, 0, 0, 0, 3, 0, 0, 0, 0]
+    got = d_out.cpu().numpy()
+    assert np.array_equal(np.delete(got, 4, 0), np.delete(want, 4, 0))
+    assert (got[4] == 0).all()
+    e.close()
+
+
+@pytest.mark.slow
+def test_1gb_batch_128_sampled_parts_match_oracle(gpu, oracle, svc, eng):
+    # 32768 records x 32 KB (1 GiB), one batch of 128: every response against the reference engine when this host
+    # can run it, and a seeded sample of response parts against the oracle restatement.
+    from oracle.oracle import RefEngine, ref_methods
+    p, st, e = _engine(svc, eng, 32768, 32768, 31)
+    b = 128
+    req = svc.synthetic_requests(p, b, seed=32)
+    frames_ = [req[i] for i in range(b)]
+    n, status, out = _answer(e, frames_)
+    assert n == b and (status == 0).all()
+    rng = np.random.default_rng(33)
+    part = st.prefixes[0].size
+    for c, o in zip(rng.integers(0, b, 10), rng.integers(0, p.instances, 10)):
+        want = oracle.answer_part(st, frames_[c], int(o))
+        assert np.array_equal(out[c, o * part:(o + 1) * part], want), (c, o)
+    methods = ref_methods()
+    if methods:
+        ref = RefEngine(st)
+        rr, rs, rout, _ = ref.answer(frames_, methods[0])
+        assert rr == b and np.array_equal(rout, out)
+        ref.close()
+    e.close()
