@@ -35,6 +35,8 @@ void set_error(const std::string &msg) { g_last_error = msg; }
   } while (0)
 
 constexpr size_t kSlotLead = 7;  // frame offset inside a staging slot: puts the key words on a 16-byte boundary
+constexpr int kMarks = 7;          // timing marks per batch (see enqueue_batch)
+constexpr int kTimingSets = 128;   // batches that may be in flight with timing marks
 
 // ------------------------------------------------------------------------------------------- tensor maps
 using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -99,10 +101,52 @@ struct Engine {
   uint32_t *d_acc = nullptr, *d_beta = nullptr;
   int *h_status = nullptr;
   uint32_t *h_err = nullptr;
-  cudaEvent_t ev[6] = {};
+  // per call: before the uploads, after the downloads
+  cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
+  // per batch: a ring of kMarks timing marks, accumulated into kernel_ms when the stream is synchronised
+  cudaEvent_t marks[kTimingSets][kMarks] = {};
+  int mark_next = 0, last_set = 0;
+  std::vector<int> pending;
+  double kernel_ms[5] = {0, 0, 0, 0, 0};  // validate, limb split + zeroing, scan, pack, tail
+  long long kernel_batches = 0;
   CUtensorMap map_db, map_ub;
   int last_launches = 0;
 };
+
+// Adds the kernel intervals of one recorded timing set to the engine's totals (its last mark must have completed).
+bool accumulate(Engine *e, int set) {
+  float t[kMarks - 1];
+  for (int i = 0; i + 1 < kMarks; ++i) ALTO_CK(cudaEventElapsedTime(&t[i], e->marks[set][i], e->marks[set][i + 1]));
+  e->kernel_ms[0] += t[0];          // validate (+ status copy)
+  e->kernel_ms[1] += t[1] + t[3];   // query limb split + accumulator zeroing, key limb split
+  e->kernel_ms[2] += t[2];          // scan GEMM
+  e->kernel_ms[3] += t[4];          // pack GEMM
+  e->kernel_ms[4] += t[5];          // tail
+  e->kernel_batches += 1;
+  return true;
+}
+
+bool accumulate_pending(Engine *e) {
+  for (int set : e->pending)
+    if (!accumulate(e, set)) return false;
+  e->pending.clear();
+  return true;
+}
+
+// The next timing set; when the ring is full the oldest pending set is waited for and accumulated first.
+bool next_set(Engine *e, int *set) {
+  *set = e->mark_next;
+  e->mark_next = (e->mark_next + 1) % kTimingSets;
+  auto it = std::find(e->pending.begin(), e->pending.end(), *set);
+  if (it != e->pending.end()) {
+    ALTO_CK(cudaEventSynchronize(e->marks[*set][kMarks - 1]));
+    if (!accumulate(e, *set)) return false;
+    e->pending.erase(it);
+  }
+  e->pending.push_back(*set);
+  e->last_set = *set;
+  return true;
+}
 
 void free_scratch(Engine *e) {
   cudaFree(e->d_req);
@@ -132,8 +176,11 @@ void destroy(Engine *e) {
   cudaFree(e->d_tw);
   cudaFree(e->d_err);
   cudaFreeHost(e->h_err);
-  for (cudaEvent_t &ev : e->ev)
-    if (ev) cudaEventDestroy(ev);
+  if (e->ev_begin) cudaEventDestroy(e->ev_begin);
+  if (e->ev_end) cudaEventDestroy(e->ev_end);
+  for (auto &set : e->marks)
+    for (cudaEvent_t &ev : set)
+      if (ev) cudaEventDestroy(ev);
   if (e->st) cudaStreamDestroy(e->st);
   delete e;
 }
@@ -219,13 +266,18 @@ bool enqueue_batch(Engine *e, const uint8_t *d_slots, size_t slot_stride, size_t
   const Plan p = make_plan(e, slots);
   const int bp = (int)round_up(slots, 4);
   int launches = 0;
+  int set = 0;
+  if (!next_set(e, &set)) return false;
+  cudaEvent_t *mk = e->marks[set];
+  // marks: 0 begin | validate | 1 | q split, zeroing | 2 | scan | 3 | y split | 4 | pack | 5 | tail | 6
+  ALTO_CK(cudaEventRecord(mk[0], st));
 
   alto::validate_kernel<<<(unsigned)slots, 256, 0, st>>>(d_slots, slot_stride, kSlotLead, e->count, e->rows,
                                                          e->d_status);
   ++launches;
   ALTO_CK(cudaGetLastError());
   if (host_status) ALTO_CK(cudaMemcpyAsync(e->h_status, e->d_status, slots * sizeof(int), cudaMemcpyDeviceToHost, st));
-  ALTO_CK(cudaEventRecord(e->ev[1], st));
+  ALTO_CK(cudaEventRecord(mk[1], st));
 
   const unsigned split_threads = 256;
   {
@@ -239,6 +291,7 @@ bool enqueue_batch(Engine *e, const uint8_t *d_slots, size_t slot_stride, size_t
   CUtensorMap map_q, map_y;
   if (!make_map(&map_q, e->d_qlimb, e->rows, 4 * (uint64_t)bp, e->rows, (uint32_t)p.bn)) return false;
   if (!make_map(&map_y, e->d_ylimb, e->count, 4 * (uint64_t)bp, e->count, (uint32_t)p.bn)) return false;
+  ALTO_CK(cudaEventRecord(mk[2], st));
   {
     alto::GemmArgs g;
     g.num_m = p.scan_m;
@@ -254,7 +307,7 @@ bool enqueue_batch(Engine *e, const uint8_t *d_slots, size_t slot_stride, size_t
       return false;
     ++launches;
   }
-  ALTO_CK(cudaEventRecord(e->ev[2], st));
+  ALTO_CK(cudaEventRecord(mk[3], st));
   {
     const size_t work = (e->count / 16) * (size_t)bp;
     alto::limb_split_kernel<<<(unsigned)((work + split_threads - 1) / split_threads), split_threads, 0, st>>>(
@@ -262,6 +315,7 @@ bool enqueue_batch(Engine *e, const uint8_t *d_slots, size_t slot_stride, size_t
     ++launches;
     ALTO_CK(cudaGetLastError());
   }
+  ALTO_CK(cudaEventRecord(mk[4], st));
   {
     alto::GemmArgs g;
     g.num_m = p.pack_m;
@@ -276,7 +330,7 @@ bool enqueue_batch(Engine *e, const uint8_t *d_slots, size_t slot_stride, size_t
     if (!dispatch_gemm<alto::Epi::kPack>(p.bn, e->map_ub, map_y, g, p.pack_m * p.num_n, st)) return false;
     ++launches;
   }
-  ALTO_CK(cudaEventRecord(e->ev[3], st));
+  ALTO_CK(cudaEventRecord(mk[5], st));
   {
     alto::TailArgs t;
     t.acc = e->d_acc;
@@ -304,7 +358,7 @@ bool enqueue_batch(Engine *e, const uint8_t *d_slots, size_t slot_stride, size_t
     ++launches;
     ALTO_CK(cudaGetLastError());
   }
-  ALTO_CK(cudaEventRecord(e->ev[4], st));
+  ALTO_CK(cudaEventRecord(mk[6], st));
   e->last_launches = launches;
   return true;
 }
@@ -338,23 +392,37 @@ bool copy_runs(size_t items, size_t width, SrcAt src_at, DstAt dst_at, cudaMemcp
   return true;
 }
 
-bool finish(Engine *e, double *stage_ms, int launches_extra) {
-  (void)launches_extra;
+// Waits for the engine's stream, folds pending timing marks into the totals and checks (then clears) the device
+// error word.
+bool sync_engine(Engine *e) {
   ALTO_CK(cudaMemcpyAsync(e->h_err, e->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->st));
   ALTO_CK(cudaStreamSynchronize(e->st));
-  if (*e->h_err) {
+  const uint32_t err = *e->h_err;
+  if (err) {
+    ALTO_CK(cudaMemsetAsync(e->d_err, 0, sizeof(uint32_t), e->st));
+    ALTO_CK(cudaStreamSynchronize(e->st));
     char buf[96];
-    snprintf(buf, sizeof buf, "a kernel wait timed out (device error word 0x%x)", *e->h_err);
+    snprintf(buf, sizeof buf, "a kernel wait timed out (device error word 0x%x)", err);
     set_error(buf);
     return false;
   }
+  return accumulate_pending(e);
+}
+
+bool finish(Engine *e, double *stage_ms) {
+  const int set = e->last_set;
+  if (!sync_engine(e)) return false;
   if (stage_ms) {
-    float t[5];
-    for (int i = 0; i < 5; ++i) ALTO_CK(cudaEventElapsedTime(&t[i], e->ev[0], e->ev[i + 1]));
-    stage_ms[0] = t[0];
-    stage_ms[1] = t[1] - t[0];
-    stage_ms[2] = t[2] - t[1];
-    stage_ms[3] = t[4] - t[2];
+    float a, b, c, d;
+    cudaEvent_t *mk = e->marks[set];
+    ALTO_CK(cudaEventElapsedTime(&a, e->ev_begin, mk[1]));
+    ALTO_CK(cudaEventElapsedTime(&b, mk[1], mk[3]));
+    ALTO_CK(cudaEventElapsedTime(&c, mk[3], mk[5]));
+    ALTO_CK(cudaEventElapsedTime(&d, mk[5], e->ev_end));
+    stage_ms[0] = a;
+    stage_ms[1] = b;
+    stage_ms[2] = c;
+    stage_ms[3] = d;
   }
   return true;
 }
@@ -398,14 +466,13 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
   }
   if (cudaSetDevice(e->dev) != cudaSuccess || !ensure_capacity(e, cand.size())) return -4;
   cudaStream_t st = e->st;
-  if (cudaMemsetAsync(e->d_err, 0, sizeof(uint32_t), st) != cudaSuccess) return -4;
-  if (cudaEventRecord(e->ev[0], st) != cudaSuccess) return -4;
+  if (cudaEventRecord(e->ev_begin, st) != cudaSuccess) return -4;
   if (!copy_runs(
           cand.size(), e->want, [&](size_t i) { return (const void *)req[cand[i]]; },
           [&](size_t i) { return (void *)(e->d_req + i * e->slot_stride + kSlotLead); }, cudaMemcpyHostToDevice, st))
     return -4;
   if (!enqueue_batch(e, e->d_req, e->slot_stride, cand.size(), e->d_resp, e->resp_len, true)) return -4;
-  if (cudaEventSynchronize(e->ev[1]) != cudaSuccess) {
+  if (cudaEventSynchronize(e->marks[e->last_set][1]) != cudaSuccess) {
     set_error("status event failed");
     return -4;
   }
@@ -418,8 +485,8 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
           ok.size(), e->resp_len, [&](size_t k) { return (const void *)(e->d_resp + ok[k] * e->resp_len); },
           [&](size_t k) { return (void *)out[cand[ok[k]]]; }, cudaMemcpyDeviceToHost, st))
     return -4;
-  if (cudaEventRecord(e->ev[5], st) != cudaSuccess) return -4;
-  if (!finish(e, stage_ms, 0)) return -4;
+  if (cudaEventRecord(e->ev_end, st) != cudaSuccess) return -4;
+  if (!finish(e, stage_ms)) return -4;
   return (int)ok.size();
 }
 
@@ -483,8 +550,11 @@ void *alto_engine_new(const uint8_t *db_col, const uint8_t *db_tiled, size_t ld,
   cudaError_t err;
   if ((err = cudaGetDevice(&e->dev)) != cudaSuccess) return fail("cudaGetDevice", err);
   if ((err = cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking)) != cudaSuccess) return fail("stream", err);
-  for (cudaEvent_t &ev : e->ev)
-    if ((err = cudaEventCreate(&ev)) != cudaSuccess) return fail("event", err);
+  if ((err = cudaEventCreate(&e->ev_begin)) != cudaSuccess || (err = cudaEventCreate(&e->ev_end)) != cudaSuccess)
+    return fail("event", err);
+  for (auto &set : e->marks)
+    for (cudaEvent_t &ev : set)
+      if ((err = cudaEventCreate(&ev)) != cudaSuccess) return fail("event", err);
   if ((err = cudaMalloc(&e->d_db, rows * cols)) != cudaSuccess) return fail("database", err);
   if ((err = cudaMemcpy2D(e->d_db, rows, db_col, ld, rows, cols, cudaMemcpyHostToDevice)) != cudaSuccess)
     return fail("database upload", err);
@@ -551,17 +621,57 @@ int alto_answer_device(void *p, const uint8_t *d_req, size_t req_stride, size_t 
   if (!b) return 0;
   if (!e->tail_ok) return -3;
   if (cudaSetDevice(e->dev) != cudaSuccess || !ensure_capacity(e, b)) return -4;
-  if (cudaMemsetAsync(e->d_err, 0, sizeof(uint32_t), e->st) != cudaSuccess) return -4;
-  if (cudaEventRecord(e->ev[0], e->st) != cudaSuccess) return -4;
+  if (cudaEventRecord(e->ev_begin, e->st) != cudaSuccess) return -4;
   if (!enqueue_batch(e, d_req, req_stride, b, d_out, out_stride, true)) return -4;
-  if (cudaEventRecord(e->ev[5], e->st) != cudaSuccess) return -4;
-  if (!finish(e, stage_ms, 0)) return -4;
+  if (cudaEventRecord(e->ev_end, e->st) != cudaSuccess) return -4;
+  if (!finish(e, stage_ms)) return -4;
   int valid = 0;
   for (size_t c = 0; c < b; ++c) {
     status[c] = e->h_status[c];
     valid += status[c] == 0;
   }
   return valid;
+}
+
+int alto_enqueue_device(void *p, const uint8_t *d_req, size_t req_stride, size_t b, uint8_t *d_out, size_t out_stride,
+                        int *d_status) {
+  Engine *e = static_cast<Engine *>(p);
+  if (!e || !d_req || !d_out || req_stride % 16 || req_stride < round_up(kSlotLead + e->want, 16) ||
+      out_stride < e->resp_len)
+    return -1;
+  e->last_launches = 0;
+  if (!b) return 0;
+  if (!e->tail_ok) return -3;
+  if (cudaSetDevice(e->dev) != cudaSuccess || !ensure_capacity(e, b)) return -4;
+  if (!enqueue_batch(e, d_req, req_stride, b, d_out, out_stride, false)) return -4;
+  if (d_status &&
+      cudaMemcpyAsync(d_status, e->d_status, b * sizeof(int), cudaMemcpyDeviceToDevice, e->st) != cudaSuccess) {
+    set_error("status copy failed");
+    return -4;
+  }
+  return 0;
+}
+
+int alto_engine_sync(void *p) {
+  Engine *e = static_cast<Engine *>(p);
+  if (!e) return -1;
+  if (cudaSetDevice(e->dev) != cudaSuccess) return -4;
+  return sync_engine(e) ? 0 : -4;
+}
+
+void *alto_engine_stream(void *p) { return p ? static_cast<void *>(static_cast<Engine *>(p)->st) : nullptr; }
+
+int alto_kernel_times(void *p, double *ms, long long *batches, int reset) {
+  Engine *e = static_cast<Engine *>(p);
+  if (!e || !ms) return -1;
+  if (cudaSetDevice(e->dev) != cudaSuccess || !sync_engine(e)) return -4;
+  for (int i = 0; i < 5; ++i) ms[i] = e->kernel_ms[i];
+  if (batches) *batches = e->kernel_batches;
+  if (reset) {
+    std::fill(e->kernel_ms, e->kernel_ms + 5, 0.0);
+    e->kernel_batches = 0;
+  }
+  return 0;
 }
 
 int alto_last_launches(const void *p) { return p ? static_cast<const Engine *>(p)->last_launches : 0; }

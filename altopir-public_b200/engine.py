@@ -123,6 +123,31 @@ class Engine:
         return lib().alto_answer_device(self.ptr, ctypes.c_void_p(d_req), req_stride, b, ctypes.c_void_p(d_out),
                                         out_stride, status.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), stage)
 
+    def enqueue_device(self, d_req, req_stride, b, d_out, out_stride, d_status=None):
+        """alto_enqueue_device: enqueue without waiting; check completion with sync()."""
+        r = lib().alto_enqueue_device(self.ptr, ctypes.c_void_p(d_req), req_stride, b, ctypes.c_void_p(d_out),
+                                      out_stride, ctypes.c_void_p(d_status) if d_status else None)
+        if r < 0:
+            raise EngineError(f"engine error {r}: {last_error()}")
+
+    def sync(self):
+        r = lib().alto_engine_sync(self.ptr)
+        if r < 0:
+            raise EngineError(f"engine error {r}: {last_error()}")
+
+    def stream(self):
+        """The engine's cudaStream_t as an integer handle (torch.cuda.ExternalStream accepts it)."""
+        return lib().alto_engine_stream(self.ptr)
+
+    def kernel_times(self, reset=True):
+        """(ms summed per kernel [validate, split, scan, pack, tail], batches) since the last reset."""
+        ms = (ctypes.c_double * 5)()
+        nb = ctypes.c_longlong(0)
+        r = lib().alto_kernel_times(self.ptr, ms, ctypes.byref(nb), int(reset))
+        if r < 0:
+            raise EngineError(f"engine error {r}: {last_error()}")
+        return list(ms), nb.value
+
     def last_launches(self):
         return lib().alto_last_launches(self.ptr)
 

@@ -1,0 +1,398 @@
+#!/usr/bin/env python
+"""Throughput of the AltoPIR answer path on B200: byte-exact QPS of 128-query batches on a 1 GiB database
+(32,768 records x 32 KB), the configuration the reference's headline batch numbers are quoted on.
+
+One step = one batch of --batch queries through the whole answer path (validate, limb split, scan, pack, tail).
+  value : device-resident throughput -- frames already in HBM, batches enqueued back to back on the engine's
+          stream (alto_enqueue_device), timed with CUDA events on that stream, max over ranks.
+  e2e   : the same metric through the reference-facing C ABI (alto_answer) with pinned HOST frames and output
+          buffers: every step uploads its frames and downloads its responses inside the timed region.
+Every rank answers its own batches on its own GPU (the answer path needs no exchange between GPUs: replicas, weak
+scaling).  `--impl reference` runs the reference's CPU engine (src/amx_kernels.cpp compiled from its own sources,
+AMX when the host has it) on the same workload, on rank 0 only.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "QPS (byte-exact) at 1/8/64 GB DB, batched vs per-query on 1 B200; p50/p99 ms"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--rows", type=int, default=32768)
+    ap.add_argument("--record-bytes", type=int, default=32768)
+    ap.add_argument("--batch", type=int, default=128)
+    ap.add_argument("--plain-queries", type=int, default=128, help="single-query launches timed for the plain path")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def config_dict(a):
+    gib = a.rows * a.record_bytes / 2 ** 30
+    return {"workload": f"answer {a.batch}-query batches over a {gib:g} GiB database ({a.rows} records x "
+                        f"{a.record_bytes} B), synthetic records of the reference generator, seeded keys/queries",
+            "rows": a.rows, "record_bytes": a.record_bytes, "batch": a.batch, "n": 2048, "tg": 4,
+            "l2": "inputs larger than L2: every step streams the 1 GiB database and the 1 GiB packing matrix"}
+
+
+# ------------------------------------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms while running."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self):
+        self.samples = []
+        self.proc = None
+        self.marks = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        threading.Thread(target=self._read, daemon=True).start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append((time.time(), [x.strip() for x in line.split(",")]))
+
+    def mark(self, t0, t1):
+        self.marks.append((t0, t1))
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        inside = [s for t, s in self.samples if any(a - 0.25 <= t <= b + 0.25 for a, b in self.marks)]
+        use = inside or [s for _, s in self.samples]
+        if not use:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no nvidia-smi samples"], "samples": 0}
+        sm = [float(s[1]) for s in use if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in use if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in use for i in range(4) if len(s) > 5 + i and s[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(use), "in_timed_region": bool(inside)}
+
+
+# ------------------------------------------------------------------------------------------------ helpers
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def algorithmic(rows, cols, b, count):
+    """Per-batch algorithmic work of the two limb GEMMs: int8 ops (1 multiply-add = 2) and compulsory bytes."""
+    return {
+        "scan_gemm": {"ops": 2.0 * cols * rows * 4 * b, "bytes": rows * cols + rows * 4 * b + 4 * b * cols},
+        "pack_gemm": {"ops": 2.0 * 4 * cols * count * 4 * b, "bytes": 4 * count * cols + 4 * count * b + 4 * b * cols},
+    }
+
+
+def int8_cublas_tops(torch):
+    """Dense int8 GEMM throughput of cuBLASLt (torch._int_mm, 8192^3) on this GPU, best of 10: context only."""
+    try:
+        a = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda")
+        b = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda")
+        for _ in range(3):
+            torch._int_mm(a, b)
+        best = 1e9
+        for _ in range(10):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            torch._int_mm(a, b)
+            e.record()
+            e.synchronize()
+            best = min(best, s.elapsed_time(e))
+        del a, b
+        return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+    except Exception:  # noqa: BLE001 -- informational only
+        return None
+
+
+def traffic_from_profile(kernel):
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(kernel, {}).get("dram_bytes_per_launch")
+    except OSError:
+        return None
+
+
+# ------------------------------------------------------------------------------------------------ reference arm
+def reference_state(a, svc):
+    p = svc.params(a.rows, a.record_bytes)
+    return p, svc.SyntheticState.make(p, seed=1, keep_values=True)
+
+
+def run_reference_cpu(a, svc, orc, st, frames, steps, warmup):
+    """Times the reference engine (or the oracle port when the host cannot run it) on batches of a.batch frames.
+    Returns (qps, info, first_out)."""
+    methods = orc.ref_methods()
+    threads = os.cpu_count() or 1
+    fl = [frames[i] for i in range(len(frames))]
+    if methods:
+        ref = orc.RefEngine(st, threads=threads)
+        m = methods[0]
+        first = None
+        for i in range(warmup):
+            r, status, out, _ = ref.answer(fl, m)
+            first = out if first is None else first
+        times = []
+        for i in range(steps):
+            t0 = time.perf_counter()
+            r, status, out, _ = ref.answer(fl, m)
+            times.append(time.perf_counter() - t0)
+            first = out if first is None else first
+            assert r == len(fl)
+        ref.close()
+        kind = "reference"
+        name = "reference engine src/amx_kernels.cpp (" + ("AMX" if m == 0 else "AVX-512 VNNI") + ")"
+        qps = len(fl) * len(times) / sum(times)
+        return qps, {"kind": kind, "cores": threads, "engine": name,
+                     "sample": f"{steps} timed batches of {len(fl)} queries after {warmup} warm-up, 1 GiB state",
+                     "median_batch_ms": 1e3 * statistics.median(times)}, first
+    # no AVX-512: the plain-C restatement, on a bounded sample of queries
+    o = orc.Oracle()
+    sub = fl[:8]
+    t0 = time.perf_counter()
+    r, status, out = o.answer(st, sub)
+    dt = time.perf_counter() - t0
+    return len(sub) / dt, {"kind": "port", "cores": threads, "engine": "oracle/alto_oracle.c",
+                           "sample": f"one batch of {len(sub)} queries"}, None
+
+
+def main_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import __graft_entry__ as ge
+    ge.load()
+    from altopir_b200 import service as svc
+    from oracle import oracle as orc
+    p, st = reference_state(a, svc)
+    frames = svc.synthetic_requests(p, a.batch, seed=1000)
+    steps, warmup = max(1, a.steps), max(1, a.warmup)
+    # bound the CPU arm to a few minutes: one batch takes ~0.1-0.3 s on 16 AMX cores
+    steps = min(steps, 40)
+    warmup = min(warmup, 3)
+    qps, info, _ = run_reference_cpu(a, svc, orc, st, frames, steps, warmup)
+    line = {"impl": "reference", "metric": METRIC, "value": qps, "unit": "QPS", "n_gpus": a.gpus, "steps": steps,
+            "warmup": warmup, "ms_per_step": 1e3 * a.batch / qps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8 x u32 limbs -> int32/u64 (exact integer)", "data": "synthetic",
+            "config": config_dict(a), "cpu_baseline": dict(info, value=qps, unit="QPS"),
+            "e2e": {"value": qps, "unit": "QPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------------------------------------ our arm
+def main_ours(a):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    import __graft_entry__ as ge
+    ge.load()
+    from altopir_b200 import engine as eng, service as svc
+
+    eng.init()
+    p = svc.params(a.rows, a.record_bytes)
+    want_cpu = rank == 0 and world == 1 and not a.no_cpu_baseline
+    st = svc.SyntheticState.make(p, seed=1, keep_values=want_cpu)
+    e = eng.Engine.from_state(st, threads=svc.threads())
+    if not want_cpu:
+        st.ub = None
+    B, rl, ql = a.batch, e.response_len(), e.request_len()
+    frames = svc.synthetic_requests(p, B, seed=1000 + rank)
+
+    # device-resident frames: frame c at slots[c, 7:7 + ql] (the engine's staged layout)
+    stride = (7 + ql + 255) // 256 * 256
+    slots = torch.zeros((B, stride), dtype=torch.uint8, device="cuda")
+    slots[:, 7:7 + ql] = torch.from_numpy(frames).cuda()
+    d_out = torch.zeros((B, rl), dtype=torch.uint8, device="cuda")
+    d_status = torch.full((B,), -1, dtype=torch.int32, device="cuda")
+    # pinned host frames and outputs for the end-to-end path
+    h_req = torch.from_numpy(frames).pin_memory()
+    h_out = torch.zeros((B, rl), dtype=torch.uint8).pin_memory()
+    req_ptrs = (ctypes.c_void_p * B)(*[h_req.data_ptr() + c * ql for c in range(B)])
+    lens = (ctypes.c_size_t * B)(*([ql] * B))
+    out_ptrs = (ctypes.c_void_p * B)(*[h_out.data_ptr() + c * rl for c in range(B)])
+    h_status = np.full(B, -1, dtype=np.int32)
+    stream = torch.cuda.ExternalStream(e.stream())
+
+    peaks, peak_src = measured_peaks()
+    int8_tops = int8_cublas_tops(torch) if rank == 0 else None
+    sampler = ClockSampler()
+    if rank == 0:
+        sampler.start()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- warm-up (both paths)
+    for _ in range(max(3, a.warmup)):
+        e.enqueue_device(slots.data_ptr(), stride, B, d_out.data_ptr(), rl, d_status.data_ptr())
+    e.sync()
+    for _ in range(max(3, a.warmup)):
+        r = e.answer_raw(req_ptrs, lens, B, out_ptrs, h_status)
+        assert r == B, (r, eng.last_error())
+
+    # ---- value: device-resident batches back to back
+    e.kernel_times(reset=True)
+    barrier()
+    torch.cuda.synchronize()
+    e.sync()
+    s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.time()
+    s_ev.record(stream)
+    for _ in range(a.steps):
+        e.enqueue_device(slots.data_ptr(), stride, B, d_out.data_ptr(), rl, d_status.data_ptr())
+    e_ev.record(stream)
+    e.sync()
+    torch.cuda.synchronize()
+    t1 = time.time()
+    sampler.mark(t0, t1)
+    value_ms = max_over_ranks(s_ev.elapsed_time(e_ev))
+    kms, nb = e.kernel_times(reset=True)
+    launches = e.last_launches() * a.steps
+    assert (d_status == 0).all().item()
+    dev_out = d_out.cpu().numpy()
+
+    # ---- e2e: the C ABI with host buffers (uploads and downloads inside the timed region)
+    barrier()
+    torch.cuda.synchronize()
+    s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.time()
+    s2.record(stream)
+    for _ in range(a.steps):
+        r = e.answer_raw(req_ptrs, lens, B, out_ptrs, h_status)
+        if r != B:
+            raise RuntimeError(f"alto_answer returned {r}: {eng.last_error()}")
+    e2.record(stream)
+    torch.cuda.synchronize()
+    t1 = time.time()
+    sampler.mark(t0, t1)
+    e2e_ms = max_over_ranks(s2.elapsed_time(e2))
+    host_out = h_out.numpy().copy()
+    e.kernel_times(reset=True)
+
+    # ---- the plain path: one query per launch, each waited for
+    lat = []
+    one = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    for i in range(a.plain_queries):
+        c = i % B
+        one[0].record(stream)
+        e.enqueue_device(slots[c].data_ptr(), stride, 1, d_out[c].data_ptr(), rl, None)
+        one[1].record(stream)
+        e.sync()
+        lat.append(one[0].elapsed_time(one[1]))
+    plain_total = max_over_ranks(sum(lat))
+    sampler.stop()
+
+    byte_exact_paths = bool(np.array_equal(dev_out, host_out))
+
+    # ---- roofline of the dominant kernel (CUDA events on the engine stream over the timed region)
+    alg = algorithmic(p.rows, p.record_bytes, B, p.count)
+    avg = {"scan_gemm": kms[2] / max(nb, 1), "pack_gemm": kms[3] / max(nb, 1)}
+    dom = max(avg, key=avg.get)
+    int8_peak = 2.0 * peaks["bf16_tflops"]
+    kernels = {}
+    for k, ms in avg.items():
+        kernels[k] = {"avg_ms": ms, "tops": alg[k]["ops"] / (ms * 1e-3) / 1e12,
+                      "gbs": alg[k]["bytes"] / (ms * 1e-3) / 1e9}
+    kernels["validate"] = {"avg_ms": kms[0] / max(nb, 1)}
+    kernels["limb_split"] = {"avg_ms": kms[1] / max(nb, 1)}
+    kernels["tail"] = {"avg_ms": kms[4] / max(nb, 1)}
+    traffic = traffic_from_profile(dom)
+    roofline = {"kernel": dom, "bound": "tensor", "achieved": kernels[dom]["tops"], "peak": int8_peak,
+                "unit": "TFLOP/s", "frac": kernels[dom]["tops"] / int8_peak, "traffic": traffic,
+                "peak_source": f"2 x {peak_src} dense bf16 ({peaks['bf16_tflops']} TF/s; B200 int8 dense rate = 2x "
+                               f"bf16); int8 ops counted as 2 per multiply-add",
+                "hbm_view": {"achieved_gbs": kernels[dom]["gbs"], "peak_gbs": peaks["hbm_gbs"],
+                             "frac": kernels[dom]["gbs"] / peaks["hbm_gbs"]},
+                "int8_cublaslt_tops": int8_tops, "algorithmic_bytes": alg[dom]["bytes"],
+                "algorithmic_ops": alg[dom]["ops"]}
+
+    cpu_baseline = None
+    exact_vs_ref = None
+    if want_cpu:
+        from oracle import oracle as orc
+        del e
+        qps_cpu, info, ref_out = run_reference_cpu(a, svc, orc, st, frames, steps=5, warmup=1)
+        cpu_baseline = dict(info, value=qps_cpu, unit="QPS")
+        if ref_out is not None:
+            exact_vs_ref = bool(np.array_equal(ref_out, dev_out))
+
+    if rank == 0:
+        value = world * B * a.steps / (value_ms * 1e-3)
+        e2e = world * B * a.steps / (e2e_ms * 1e-3)
+        lat_sorted = sorted(lat)
+        line = {
+            "metric": METRIC, "value": value, "unit": "QPS", "n_gpus": world, "steps": a.steps,
+            "warmup": max(3, a.warmup), "ms_per_step": value_ms / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8 x u8 limbs -> int32 (tcgen05 kind::i8), exact",
+            "data": "synthetic", "config": dict(config_dict(a), parallelism=f"replicas{world}"),
+            "e2e": {"value": e2e, "unit": "QPS", "h2d_bytes_per_step": B * ql, "d2h_bytes_per_step": B * rl + 4 * B,
+                    "ms_per_step": e2e_ms / a.steps, "api": "alto_answer (pinned host frames and outputs)"},
+            "gpu_launches": launches,
+            "roofline": roofline,
+            "kernels": kernels,
+            "cpu_baseline": cpu_baseline,
+            "clocks": sampler.summary(),
+            "plain_per_query": {"qps": world * a.plain_queries / (plain_total * 1e-3),
+                                "p50_ms": lat_sorted[len(lat) // 2], "p99_ms": lat_sorted[int(len(lat) * 0.99)],
+                                "batched_over_plain": value / (world * a.plain_queries / (plain_total * 1e-3))},
+            "byte_exact": {"device_vs_host_path": byte_exact_paths, "vs_reference_engine": exact_vs_ref},
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    args = parse()
+    sys.exit(main_reference(args) if args.impl == "reference" else main_ours(args))

@@ -94,8 +94,26 @@ const char *alto_last_error(void);
 int alto_answer_device(void *engine, const uint8_t *d_req, size_t req_stride, size_t b, uint8_t *d_out,
                        size_t out_stride, int *status, double *stage_ms);
 
-/* Counts of kernel launches issued by the most recent alto_answer / alto_answer_device call of this engine. */
+/* Count of kernel launches issued by the most recent batch of this engine. */
 int alto_last_launches(const void *engine);
+
+/* Asynchronous form of alto_answer_device: enqueues the whole batch on the engine's stream and returns at once
+ * (0, or -1/-3/-4 as alto_answer).  Statuses are written to the device array d_status[b] when it is not NULL.
+ * Completion and kernel wait failures are reported by alto_engine_sync. */
+int alto_enqueue_device(void *engine, const uint8_t *d_req, size_t req_stride, size_t b, uint8_t *d_out,
+                        size_t out_stride, int *d_status);
+
+/* Waits for every batch enqueued on this engine; returns 0, or -4 when a kernel wait timed out since the last
+ * check (the device error word is cleared). */
+int alto_engine_sync(void *engine);
+
+/* The cudaStream_t the engine launches its kernels on (for events and stream ordering in the caller). */
+void *alto_engine_stream(void *engine);
+
+/* Device time in ms summed over the batches since the last reset, measured with CUDA events on the engine's
+ * stream: ms[0] validate, ms[1] limb split + accumulator zeroing, ms[2] scan GEMM, ms[3] pack GEMM, ms[4] tail;
+ * *batches receives the number of batches.  Synchronises the engine.  Returns 0, or -4 on a device failure. */
+int alto_kernel_times(void *engine, double *ms, long long *batches, int reset);
 
 /* Deterministic synthetic inputs (test and benchmark data; not part of the answer path).
  * alto_synthetic_db_col: db[(col - col0) * ld + r] = byte col of the reference's synthetic record r
