@@ -689,3 +689,4 @@ int alto_synthetic_db_col_device(uint8_t *d_db, size_t ld, size_t rows, size_t c
 }
 
 }  // extern "C"
+

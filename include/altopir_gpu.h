@@ -87,10 +87,11 @@ int alto_answer(void *engine, const uint8_t *const *req, const size_t *len, size
 /* Text of the last error recorded by this library on the calling thread ("" if none). */
 const char *alto_last_error(void);
 
-/* alto_answer for frames that are already resident in device memory: frame c starts at d_req + c * req_stride
- * (full frames including the 9-byte header, req_stride >= alto_request_len and a multiple of 16; the header is
- * checked on the device), responses go to d_out + c * out_stride (device memory, out_stride >= alto_response_len),
- * statuses to the host array status[b].  Returns what alto_answer returns. */
+/* alto_answer for frames that are already resident in device memory: frame c (the full frame, header included)
+ * starts at d_req + c * req_stride + 7, which puts its key words on a 16-byte boundary; req_stride is a multiple of
+ * 16 and at least 7 + alto_request_len rounded up to 16.  The header is checked on the device.  Responses go to
+ * d_out + c * out_stride (device memory, out_stride >= alto_response_len), statuses to the host array status[b].
+ * Returns what alto_answer returns. */
 int alto_answer_device(void *engine, const uint8_t *d_req, size_t req_stride, size_t b, uint8_t *d_out,
                        size_t out_stride, int *status, double *stage_ms);
 
