@@ -8,6 +8,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -690,3 +691,180 @@ int alto_synthetic_db_col_device(uint8_t *d_db, size_t ld, size_t rows, size_t c
 
 }  // extern "C"
 
+// ============================================================================================ allocation-free answer
+// Some callers cannot allocate device memory at answer time: a server that reserves all of its GPU memory up front
+// and must not grow it while serving, code running under a memory budget enforced by a pool that does not belong
+// to this library, or a thread that must not take the allocator's locks (cudaMalloc synchronises the device).
+// For them alto_answer_device_noalloc answers device-resident frames with its per-batch scratch (statuses, byte
+// limbs of queries and keys, scan sums, pack results) in the file-scope array below instead of engine buffers
+// grown with cudaMalloc.  The array has a fixed size; every GPU that loads this library holds it until the process
+// exits.  All calls share it, so calls whose work overlaps on the GPU (on any engine of the same device) race; the
+// array keeps the previous call's contents, and the scan sums, which must start at zero, are cleared by each call.
+namespace {
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;  // 16 MiB per device
+constexpr int kNoAllocMaxDevices = 64;
+}  // namespace
+
+static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+uint8_t *g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// The device address of g_noalloc_scratch on device `dev`, which must be current.  In host code the array's name is
+// only a host-side stand-in, so the address is looked up with cudaGetSymbolAddress once per device and cached.
+bool noalloc_scratch(int dev, uint8_t **addr) {
+  if (dev < 0 || dev >= kNoAllocMaxDevices) {
+    set_error("device ordinal outside the allocation-free table");
+    return false;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void *ptr = nullptr;
+    const cudaError_t err = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (err != cudaSuccess) {
+      set_error("cudaGetSymbolAddress(g_noalloc_scratch)", err);
+      return false;
+    }
+    g_noalloc_addr[dev] = static_cast<uint8_t *>(ptr);
+  }
+  *addr = g_noalloc_addr[dev];
+  return true;
+}
+
+struct NoAllocLayout {
+  size_t status = 0, qlimb = 0, ylimb = 0, acc = 0, beta = 0, total = 0;
+};
+
+NoAllocLayout noalloc_layout(const Engine *e, size_t b) {
+  NoAllocLayout l;
+  const size_t bp = round_up(b, 4);
+  size_t off = 0;
+  l.status = off;
+  off = round_up(off + b * sizeof(int), 256);
+  l.qlimb = off;
+  off = round_up(off + 4 * bp * e->rows, 256);
+  l.ylimb = off;
+  off = round_up(off + 4 * bp * e->count, 256);
+  l.acc = off;
+  off = round_up(off + b * e->cols * sizeof(uint32_t), 256);
+  l.beta = off;
+  off = round_up(off + b * e->cols * sizeof(uint32_t), 256);
+  l.total = off;
+  return l;
+}
+
+// The launch sequence of the answer path (validate, limb splits, scan, pack, tail) on scratch carved from the
+// static array; statuses are copied to the caller's device array.
+bool enqueue_noalloc(Engine *e, uint8_t *scratch, const NoAllocLayout &l, const uint8_t *d_slots, size_t stride,
+                     size_t b, uint8_t *resp, size_t resp_stride, int *d_status) {
+  cudaStream_t st = e->st;
+  const Plan p = make_plan(e, b);
+  const int bp = (int)round_up(b, 4);
+  int *status = reinterpret_cast<int *>(scratch + l.status);
+  uint8_t *qlimb = scratch + l.qlimb, *ylimb = scratch + l.ylimb;
+  uint32_t *acc = reinterpret_cast<uint32_t *>(scratch + l.acc), *beta = reinterpret_cast<uint32_t *>(scratch + l.beta);
+  const unsigned split_threads = 256;
+
+  alto::validate_kernel<<<(unsigned)b, 256, 0, st>>>(d_slots, stride, kSlotLead, e->count, e->rows, status);
+  ALTO_CK(cudaGetLastError());
+  const size_t qwork = (e->rows / 16) * (size_t)bp;
+  alto::limb_split_kernel<<<(unsigned)((qwork + split_threads - 1) / split_threads), split_threads, 0, st>>>(
+      d_slots, stride, kSlotLead + 9 + 8 * e->count, (int)b, bp, e->rows, qlimb);
+  ALTO_CK(cudaGetLastError());
+  ALTO_CK(cudaMemsetAsync(acc, 0, b * e->cols * sizeof(uint32_t), st));  // the scan adds into these sums
+  const size_t ywork = (e->count / 16) * (size_t)bp;
+  alto::limb_split_kernel<<<(unsigned)((ywork + split_threads - 1) / split_threads), split_threads, 0, st>>>(
+      d_slots, stride, kSlotLead + 9, (int)b, bp, e->count, ylimb);
+  ALTO_CK(cudaGetLastError());
+  CUtensorMap map_q, map_y;
+  if (!make_map(&map_q, qlimb, e->rows, 4 * (uint64_t)bp, e->rows, (uint32_t)p.bn)) return false;
+  if (!make_map(&map_y, ylimb, e->count, 4 * (uint64_t)bp, e->count, (uint32_t)p.bn)) return false;
+  alto::GemmArgs g;
+  g.num_m = p.scan_m;
+  g.num_n = p.num_n;
+  g.kb_total = p.scan_kb;
+  g.kb_per_unit = p.scan_kb_per;
+  g.rows_a = (int)e->cols;
+  g.clients = (int)b;
+  g.cols = (int)e->cols;
+  g.out = acc;
+  g.err = e->d_err;
+  if (!dispatch_gemm<alto::Epi::kScan>(p.bn, e->map_db, map_q, g, p.scan_m * p.num_n * p.scan_split, st)) return false;
+  g.num_m = p.pack_m;
+  g.kb_total = p.pack_kb;
+  g.kb_per_unit = p.pack_kb;
+  g.rows_a = (int)(4 * e->cols);
+  g.out = beta;
+  if (!dispatch_gemm<alto::Epi::kPack>(p.bn, e->map_ub, map_y, g, p.pack_m * p.num_n, st)) return false;
+  alto::TailArgs t;
+  t.acc = acc;
+  t.beta = beta;
+  t.status = status;
+  t.req = d_slots;
+  t.req_stride = stride;
+  t.z_off = kSlotLead + 9 + 4 * e->count;
+  t.that = e->d_that;
+  t.twiddle = e->d_tw;
+  t.prefix = e->d_prefix;
+  t.resp = resp;
+  t.resp_stride = resp_stride;
+  t.n = (int)e->n;
+  t.tg = (int)e->tg;
+  t.outputs = (int)e->outputs;
+  t.cols = (int)e->cols;
+  t.part_len = (int)e->part_len;
+  t.row1_off = (int)e->row1_off;
+  t.q1_bits = e->q1_bits;
+  t.q1 = (int64_t)e->q1;
+  const size_t smem = (e->n + (e->part_len + 3) / 4 + 1) * sizeof(uint32_t);
+  if (smem > 48 * 1024)
+    ALTO_CK(cudaFuncSetAttribute(alto::tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  alto::tail_kernel<<<(unsigned)(b * e->outputs), 256, smem, st>>>(t);
+  ALTO_CK(cudaGetLastError());
+  ALTO_CK(cudaMemcpyAsync(d_status, status, b * sizeof(int), cudaMemcpyDeviceToDevice, st));
+  return true;
+}
+
+}  // namespace
+
+extern "C" int alto_answer_device_noalloc(void *p, const uint8_t *d_req, size_t req_stride, size_t b, uint8_t *d_out,
+                                          size_t out_stride, int *d_status) {
+  Engine *e = static_cast<Engine *>(p);
+  if (!e || !d_req || !d_out || !d_status || req_stride % 16 || req_stride < round_up(kSlotLead + e->want, 16) ||
+      out_stride < e->resp_len) {
+    set_error("bad arguments");
+    return -1;
+  }
+  if (!b) return 0;
+  if (!e->tail_ok) return -3;
+  const NoAllocLayout l = noalloc_layout(e, b);
+  if (l.total > kNoAllocScratchBytes) {
+    char buf[200];
+    snprintf(buf, sizeof buf,
+             "batch of %zu needs %zu bytes of scratch; the allocation-free entry point has %zu bytes per device",
+             b, l.total, kNoAllocScratchBytes);
+    set_error(buf);
+    return -1;
+  }
+  if (cudaSetDevice(e->dev) != cudaSuccess) return -4;
+  uint8_t *scratch = nullptr;
+  if (!noalloc_scratch(e->dev, &scratch)) return -4;
+  if (!enqueue_noalloc(e, scratch, l, d_req, req_stride, b, d_out, out_stride, d_status)) return -4;
+  // wait and check the engine's device error word (its pinned host mirror already exists)
+  if (cudaMemcpyAsync(e->h_err, e->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->st) != cudaSuccess ||
+      cudaStreamSynchronize(e->st) != cudaSuccess) {
+    set_error("allocation-free batch failed", cudaGetLastError());
+    return -4;
+  }
+  if (*e->h_err) {
+    char buf[96];
+    snprintf(buf, sizeof buf, "a kernel wait timed out (device error word 0x%x)", *e->h_err);
+    set_error(buf);
+    cudaMemsetAsync(e->d_err, 0, sizeof(uint32_t), e->st);
+    cudaStreamSynchronize(e->st);
+    return -4;
+  }
+  return 0;
+}

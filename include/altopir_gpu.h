@@ -116,6 +116,20 @@ void *alto_engine_stream(void *engine);
  * *batches receives the number of batches.  Synchronises the engine.  Returns 0, or -4 on a device failure. */
 int alto_kernel_times(void *engine, double *ms, long long *batches, int reset);
 
+/* No counterpart in the reference.  alto_answer_device without any device allocation, for callers that cannot
+ * call cudaMalloc while they serve: a server that reserves its GPU memory once at start-up and must not grow it,
+ * code that runs under a memory budget kept by an allocator it does not own, or a thread that must not stall on
+ * cudaMalloc's device-wide synchronisation.  Frames and outputs are laid out as for alto_answer_device; statuses go
+ * to the device array d_status[b].  The per-batch scratch (statuses, byte limbs, scan sums, pack results) lives in
+ * a fixed 16 MiB array inside this library, which every GPU that loads the library holds until the process exits;
+ * a batch whose scratch would exceed it is rejected with -1 and a message in alto_last_error() (at 32768 records of
+ * 32 KB that is about 36 frames).  The first call on a device looks up the array's device address (set-up done
+ * once per device), so that first call should come before any stream capture.  All calls share the array: calls
+ * whose work overlaps on the GPU race, even on different engines of the same device.  Returns 0 once the batch has
+ * completed, -1, -3 or -4 as alto_answer. */
+int alto_answer_device_noalloc(void *engine, const uint8_t *d_req, size_t req_stride, size_t b, uint8_t *d_out,
+                               size_t out_stride, int *d_status);
+
 /* Deterministic synthetic inputs (test and benchmark data; not part of the answer path).
  * alto_synthetic_db_col: db[(col - col0) * ld + r] = byte col of the reference's synthetic record r
  *   (src/service.rs:43-62, splitmix64 seed 0x416c746f504952), for r < rows and ncols columns from col0.
