@@ -55,6 +55,7 @@ def _declare(L):
         "alto_fill_bytes": (None, [P, S, U64, I]),
         "alto_synthetic_request": (None, [P, S, S, U64, U64]),
         "alto_pack_encode": (None, [P, P, S, S, I]),
+        "alto_rescale_digest": (U64, [U64, U64, U64, I]),
     }
     for name, (res, args) in sigs.items():
         f = getattr(L, name)
@@ -73,5 +74,5 @@ EXPORTS = (
     "alto_answer_device", "alto_last_launches", "alto_enqueue_device", "alto_engine_sync", "alto_engine_stream",
     "alto_kernel_times", "alto_answer_device_noalloc", "alto_synthetic_db_col", "alto_synthetic_db_col_device",
     "alto_fill_uniform_u32", "alto_fill_uniform_u64", "alto_fill_bytes", "alto_synthetic_request",
-    "alto_pack_encode",
+    "alto_pack_encode", "alto_rescale_digest",
 )

@@ -102,8 +102,9 @@ struct Engine {
   uint32_t *d_acc = nullptr, *d_beta = nullptr;
   int *h_status = nullptr;
   uint32_t *h_err = nullptr;
-  // per call: before the uploads, after the downloads
-  cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
+  // per call: before the uploads, after the downloads; the query words upload on st_copy
+  cudaEvent_t ev_begin = nullptr, ev_end = nullptr, ev_keys = nullptr, ev_queries = nullptr;
+  cudaStream_t st_copy = nullptr;
   // per batch: a ring of kMarks timing marks, accumulated into kernel_ms when the stream is synchronised
   cudaEvent_t marks[kTimingSets][kMarks] = {};
   int mark_next = 0, last_set = 0;
@@ -119,9 +120,9 @@ bool accumulate(Engine *e, int set) {
   float t[kMarks - 1];
   for (int i = 0; i + 1 < kMarks; ++i) ALTO_CK(cudaEventElapsedTime(&t[i], e->marks[set][i], e->marks[set][i + 1]));
   e->kernel_ms[0] += t[0];          // validate (+ status copy)
-  e->kernel_ms[1] += t[1] + t[3];   // query limb split + accumulator zeroing, key limb split
-  e->kernel_ms[2] += t[2];          // scan GEMM
-  e->kernel_ms[3] += t[4];          // pack GEMM
+  e->kernel_ms[1] += t[1] + t[3];   // key limb split, query limb split + scan-sum zeroing (+ any upload wait)
+  e->kernel_ms[2] += t[4];          // scan GEMM
+  e->kernel_ms[3] += t[2];          // pack GEMM
   e->kernel_ms[4] += t[5];          // tail
   e->kernel_batches += 1;
   return true;
@@ -177,8 +178,10 @@ void destroy(Engine *e) {
   cudaFree(e->d_tw);
   cudaFree(e->d_err);
   cudaFreeHost(e->h_err);
-  if (e->ev_begin) cudaEventDestroy(e->ev_begin);
-  if (e->ev_end) cudaEventDestroy(e->ev_end);
+  if (e->st_copy) cudaStreamSynchronize(e->st_copy);
+  for (cudaEvent_t ev : {e->ev_begin, e->ev_end, e->ev_keys, e->ev_queries})
+    if (ev) cudaEventDestroy(ev);
+  if (e->st_copy) cudaStreamDestroy(e->st_copy);
   for (auto &set : e->marks)
     for (cudaEvent_t &ev : set)
       if (ev) cudaEventDestroy(ev);
@@ -259,10 +262,13 @@ Plan make_plan(const Engine *e, size_t slots) {
   return p;
 }
 
-// Enqueues validate .. tail for `slots` staged frames whose statuses go to d_status.  resp/resp_stride receive the
-// response parts of valid frames.
+// Enqueues the answer path for `slots` staged frames on the engine's stream: validate, key limb split, pack GEMM,
+// then (after `queries_ready`, when the query words are still being uploaded on another stream) query limb split,
+// scan GEMM and tail.  The pack needs only the keys, so it overlaps the upload of the much larger query words.
+// Statuses go to d_status (and to the pinned host copy when host_status); responses of valid frames to
+// resp + slot * resp_stride.
 bool enqueue_batch(Engine *e, const uint8_t *d_slots, size_t slot_stride, size_t slots, uint8_t *resp,
-                   size_t resp_stride, bool host_status) {
+                   size_t resp_stride, bool host_status, cudaEvent_t queries_ready = nullptr) {
   cudaStream_t st = e->st;
   const Plan p = make_plan(e, slots);
   const int bp = (int)round_up(slots, 4);
@@ -270,7 +276,7 @@ bool enqueue_batch(Engine *e, const uint8_t *d_slots, size_t slot_stride, size_t
   int set = 0;
   if (!next_set(e, &set)) return false;
   cudaEvent_t *mk = e->marks[set];
-  // marks: 0 begin | validate | 1 | q split, zeroing | 2 | scan | 3 | y split | 4 | pack | 5 | tail | 6
+  // marks: 0 begin | validate | 1 | y split | 2 | pack | 3 | (query wait) q split, zeroing | 4 | scan | 5 | tail | 6
   ALTO_CK(cudaEventRecord(mk[0], st));
 
   alto::validate_kernel<<<(unsigned)slots, 256, 0, st>>>(d_slots, slot_stride, kSlotLead, e->count, e->rows,
@@ -280,7 +286,34 @@ bool enqueue_batch(Engine *e, const uint8_t *d_slots, size_t slot_stride, size_t
   if (host_status) ALTO_CK(cudaMemcpyAsync(e->h_status, e->d_status, slots * sizeof(int), cudaMemcpyDeviceToHost, st));
   ALTO_CK(cudaEventRecord(mk[1], st));
 
+  CUtensorMap map_q, map_y;
+  if (!make_map(&map_q, e->d_qlimb, e->rows, 4 * (uint64_t)bp, e->rows, (uint32_t)p.bn)) return false;
+  if (!make_map(&map_y, e->d_ylimb, e->count, 4 * (uint64_t)bp, e->count, (uint32_t)p.bn)) return false;
   const unsigned split_threads = 256;
+  {
+    const size_t work = (e->count / 16) * (size_t)bp;
+    alto::limb_split_kernel<<<(unsigned)((work + split_threads - 1) / split_threads), split_threads, 0, st>>>(
+        d_slots, slot_stride, kSlotLead + 9, (int)slots, bp, e->count, e->d_ylimb);
+    ++launches;
+    ALTO_CK(cudaGetLastError());
+  }
+  ALTO_CK(cudaEventRecord(mk[2], st));
+  {
+    alto::GemmArgs g;
+    g.num_m = p.pack_m;
+    g.num_n = p.num_n;
+    g.kb_total = p.pack_kb;
+    g.kb_per_unit = p.pack_kb;
+    g.rows_a = (int)(4 * e->cols);
+    g.clients = (int)slots;
+    g.cols = (int)e->cols;
+    g.out = e->d_beta;
+    g.err = e->d_err;
+    if (!dispatch_gemm<alto::Epi::kPack>(p.bn, e->map_ub, map_y, g, p.pack_m * p.num_n, st)) return false;
+    ++launches;
+  }
+  ALTO_CK(cudaEventRecord(mk[3], st));
+  if (queries_ready) ALTO_CK(cudaStreamWaitEvent(st, queries_ready, 0));
   {
     const size_t work = (e->rows / 16) * (size_t)bp;
     alto::limb_split_kernel<<<(unsigned)((work + split_threads - 1) / split_threads), split_threads, 0, st>>>(
@@ -289,10 +322,7 @@ bool enqueue_batch(Engine *e, const uint8_t *d_slots, size_t slot_stride, size_t
     ALTO_CK(cudaGetLastError());
   }
   ALTO_CK(cudaMemsetAsync(e->d_acc, 0, slots * e->cols * sizeof(uint32_t), st));
-  CUtensorMap map_q, map_y;
-  if (!make_map(&map_q, e->d_qlimb, e->rows, 4 * (uint64_t)bp, e->rows, (uint32_t)p.bn)) return false;
-  if (!make_map(&map_y, e->d_ylimb, e->count, 4 * (uint64_t)bp, e->count, (uint32_t)p.bn)) return false;
-  ALTO_CK(cudaEventRecord(mk[2], st));
+  ALTO_CK(cudaEventRecord(mk[4], st));
   {
     alto::GemmArgs g;
     g.num_m = p.scan_m;
@@ -306,29 +336,6 @@ bool enqueue_batch(Engine *e, const uint8_t *d_slots, size_t slot_stride, size_t
     g.err = e->d_err;
     if (!dispatch_gemm<alto::Epi::kScan>(p.bn, e->map_db, map_q, g, p.scan_m * p.num_n * p.scan_split, st))
       return false;
-    ++launches;
-  }
-  ALTO_CK(cudaEventRecord(mk[3], st));
-  {
-    const size_t work = (e->count / 16) * (size_t)bp;
-    alto::limb_split_kernel<<<(unsigned)((work + split_threads - 1) / split_threads), split_threads, 0, st>>>(
-        d_slots, slot_stride, kSlotLead + 9, (int)slots, bp, e->count, e->d_ylimb);
-    ++launches;
-    ALTO_CK(cudaGetLastError());
-  }
-  ALTO_CK(cudaEventRecord(mk[4], st));
-  {
-    alto::GemmArgs g;
-    g.num_m = p.pack_m;
-    g.num_n = p.num_n;
-    g.kb_total = p.pack_kb;
-    g.kb_per_unit = p.pack_kb;
-    g.rows_a = (int)(4 * e->cols);
-    g.clients = (int)slots;
-    g.cols = (int)e->cols;
-    g.out = e->d_beta;
-    g.err = e->d_err;
-    if (!dispatch_gemm<alto::Epi::kPack>(p.bn, e->map_ub, map_y, g, p.pack_m * p.num_n, st)) return false;
     ++launches;
   }
   ALTO_CK(cudaEventRecord(mk[5], st));
@@ -353,11 +360,8 @@ bool enqueue_batch(Engine *e, const uint8_t *d_slots, size_t slot_stride, size_t
     t.row1_off = (int)e->row1_off;
     t.q1_bits = e->q1_bits;
     t.q1 = (int64_t)e->q1;
-    const size_t smem = (e->n + (e->part_len + 3) / 4 + 1) * sizeof(uint32_t);
-    if (smem > 48 * 1024) ALTO_CK(cudaFuncSetAttribute(alto::tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    alto::tail_kernel<<<(unsigned)(slots * e->outputs), 256, smem, st>>>(t);
+    ALTO_CK(alto::launch_tail(t, slots, st));
     ++launches;
-    ALTO_CK(cudaGetLastError());
   }
   ALTO_CK(cudaEventRecord(mk[6], st));
   e->last_launches = launches;
@@ -416,10 +420,10 @@ bool finish(Engine *e, double *stage_ms) {
   if (stage_ms) {
     float a, b, c, d;
     cudaEvent_t *mk = e->marks[set];
-    ALTO_CK(cudaEventElapsedTime(&a, e->ev_begin, mk[1]));
-    ALTO_CK(cudaEventElapsedTime(&b, mk[1], mk[3]));
-    ALTO_CK(cudaEventElapsedTime(&c, mk[3], mk[5]));
-    ALTO_CK(cudaEventElapsedTime(&d, mk[5], e->ev_end));
+    ALTO_CK(cudaEventElapsedTime(&a, e->ev_begin, mk[1]));  // key upload + validate
+    ALTO_CK(cudaEventElapsedTime(&b, mk[3], mk[5]));        // query upload wait + query split + scan
+    ALTO_CK(cudaEventElapsedTime(&c, mk[1], mk[3]));        // key split + pack
+    ALTO_CK(cudaEventElapsedTime(&d, mk[5], e->ev_end));    // tail + download
     stage_ms[0] = a;
     stage_ms[1] = b;
     stage_ms[2] = c;
@@ -468,11 +472,23 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
   if (cudaSetDevice(e->dev) != cudaSuccess || !ensure_capacity(e, cand.size())) return -4;
   cudaStream_t st = e->st;
   if (cudaEventRecord(e->ev_begin, st) != cudaSuccess) return -4;
+  // header and keys first on the compute stream, then the query words on the copy stream, so that validation and
+  // the pack run while the queries are still uploading
+  const size_t head = 9 + 8 * e->count;
   if (!copy_runs(
-          cand.size(), e->want, [&](size_t i) { return (const void *)req[cand[i]]; },
+          cand.size(), head, [&](size_t i) { return (const void *)req[cand[i]]; },
           [&](size_t i) { return (void *)(e->d_req + i * e->slot_stride + kSlotLead); }, cudaMemcpyHostToDevice, st))
     return -4;
-  if (!enqueue_batch(e, e->d_req, e->slot_stride, cand.size(), e->d_resp, e->resp_len, true)) return -4;
+  if (cudaEventRecord(e->ev_keys, st) != cudaSuccess || cudaStreamWaitEvent(e->st_copy, e->ev_keys, 0) != cudaSuccess)
+    return -4;
+  if (!copy_runs(
+          cand.size(), e->want - head, [&](size_t i) { return (const void *)(req[cand[i]] + head); },
+          [&](size_t i) { return (void *)(e->d_req + i * e->slot_stride + kSlotLead + head); },
+          cudaMemcpyHostToDevice, e->st_copy))
+    return -4;
+  if (cudaEventRecord(e->ev_queries, e->st_copy) != cudaSuccess) return -4;
+  if (!enqueue_batch(e, e->d_req, e->slot_stride, cand.size(), e->d_resp, e->resp_len, true, e->ev_queries))
+    return -4;
   if (cudaEventSynchronize(e->marks[e->last_set][1]) != cudaSuccess) {
     set_error("status event failed");
     return -4;
@@ -551,7 +567,10 @@ void *alto_engine_new(const uint8_t *db_col, const uint8_t *db_tiled, size_t ld,
   cudaError_t err;
   if ((err = cudaGetDevice(&e->dev)) != cudaSuccess) return fail("cudaGetDevice", err);
   if ((err = cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking)) != cudaSuccess) return fail("stream", err);
-  if ((err = cudaEventCreate(&e->ev_begin)) != cudaSuccess || (err = cudaEventCreate(&e->ev_end)) != cudaSuccess)
+  if ((err = cudaStreamCreateWithFlags(&e->st_copy, cudaStreamNonBlocking)) != cudaSuccess) return fail("stream", err);
+  if ((err = cudaEventCreate(&e->ev_begin)) != cudaSuccess || (err = cudaEventCreate(&e->ev_end)) != cudaSuccess ||
+      (err = cudaEventCreateWithFlags(&e->ev_keys, cudaEventDisableTiming)) != cudaSuccess ||
+      (err = cudaEventCreateWithFlags(&e->ev_queries, cudaEventDisableTiming)) != cudaSuccess)
     return fail("event", err);
   for (auto &set : e->marks)
     for (cudaEvent_t &ev : set)
@@ -818,11 +837,7 @@ bool enqueue_noalloc(Engine *e, uint8_t *scratch, const NoAllocLayout &l, const 
   t.row1_off = (int)e->row1_off;
   t.q1_bits = e->q1_bits;
   t.q1 = (int64_t)e->q1;
-  const size_t smem = (e->n + (e->part_len + 3) / 4 + 1) * sizeof(uint32_t);
-  if (smem > 48 * 1024)
-    ALTO_CK(cudaFuncSetAttribute(alto::tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  alto::tail_kernel<<<(unsigned)(b * e->outputs), 256, smem, st>>>(t);
-  ALTO_CK(cudaGetLastError());
+  ALTO_CK(alto::launch_tail(t, b, st));
   ALTO_CK(cudaMemcpyAsync(d_status, status, b * sizeof(int), cudaMemcpyDeviceToDevice, st));
   return true;
 }

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/altopir_gpu.h"
+#include "modq.cuh"
 
 namespace {
 
@@ -161,6 +162,14 @@ void alto_synthetic_request(uint8_t *frame, size_t rows, size_t tg_n, uint64_t s
     const uint32_t v = static_cast<uint32_t>(stream_at(s, 2 * tg_n + i) >> 32);
     memcpy(w + 4 * i, &v, 4);
   }
+}
+
+uint64_t alto_rescale_digest(uint64_t q1, uint64_t v0, uint64_t v1, int threads) {
+  uint64_t d = 0;
+#pragma omp parallel for num_threads(nthreads(threads)) reduction(+ : d) schedule(static)
+  for (int64_t v = (int64_t)v0; v < (int64_t)v1; ++v)
+    d += (uint64_t)alto::rescale_q((uint32_t)v, (uint32_t)q1) * (2 * (uint64_t)v + 1);
+  return d;
 }
 
 }  // extern "C"

@@ -3,6 +3,7 @@
 #pragma once
 #include <cstdint>
 #include "limb_gemm.cuh"
+#include "modq.cuh"
 
 namespace alto {
 
@@ -72,34 +73,13 @@ __global__ void limb_split_kernel(const uint8_t *__restrict__ req, size_t stride
 }
 
 // ------------------------------------------------------------------------------------ tail
-__device__ __forceinline__ uint32_t mulmod_q(uint32_t a, uint32_t b) {
-  return (uint32_t)mod_q64((uint64_t)a * b);
-}
-__device__ __forceinline__ uint32_t addmod_q(uint32_t a, uint32_t b) {
-  const uint64_t s = (uint64_t)a + b;
-  return (uint32_t)(s >= kQ ? s - kQ : s);
-}
-
-// Centred rescale Q -> q1 with round-half-away-from-zero into [0, q1) (src/amx_kernels.cpp:522-529).  The reference
-// divides in double precision; |c * q1 +- floor(Q/2)| < 2^53 and the quotient's rounding cannot cross an integer,
-// so truncating 64-bit integer division by the constant Q gives the same integer.
-__device__ __forceinline__ uint32_t rescale_q1(uint32_t v, int64_t q1) {
-  constexpr int64_t half = (int64_t)(kQ / 2);
-  const bool neg = v >= (uint32_t)half;
-  const int64_t c = neg ? (int64_t)v - (int64_t)kQ : (int64_t)v;
-  int64_t t = (c * q1 + (neg ? -half : half)) / (int64_t)kQ;
-  if (t < 0) t += q1;
-  if (t >= q1) t -= q1;
-  return (uint32_t)t;
-}
-
 struct TailArgs {
   const uint32_t *acc;      // scan sums mod 2^32, [slot][cols]
   const uint32_t *beta;     // pack results mod Q, [slot][cols]
   const int *status;        // per-slot status; only slots with status 0 are answered
   const uint8_t *req;       // staged request bodies (y, z, q words), [slot][req_stride]
   size_t req_stride;
-  size_t z_off;             // byte offset of the z key words within a body
+  size_t z_off;             // byte offset of the z key words within a slot
   const uint32_t *that;     // bold_t_hat mod Q, [output][tg * n]
   const uint32_t *twiddle;  // inverse-NTT table, low 32 bits of each entry, [n]
   const uint8_t *prefix;    // row-0 prefixes, [output][part_len]
@@ -110,16 +90,46 @@ struct TailArgs {
   int64_t q1;
 };
 
-// One CTA per (slot, output).  Shared memory: n accumulator words, then the response part as 32-bit words.
-// acc[i] = beta + sum_k z[k n + i] * that[k n + i] (mod Q)    (src/amx_kernels.cpp:500-511)
-// inverse NTT, stages t = 1..n/2, twiddle table[n/(2t) + block], x' = (x+y)/2, y' = (x-y)w   (:461-498)
-// v = rescale(inter + acc) with inter = (acc_scan * Q + 2^31) >> 32 (:306-307, :515-529)
-// part = prefix with the q1_bits-bit values ORed in LSB-first from bit row1_off (:530-534, :605-607)
-__global__ void __launch_bounds__(256) tail_kernel(TailArgs a) {
+// One response part per CTA (slot, output o), n / 8 threads owning 8 coefficients each.
+//   acc[i] = beta[i] + sum_k z[k n + i] * that[k n + i] (mod Q)                    (src/amx_kernels.cpp:500-511)
+//   inverse NTT: stages t = 1, 2, ..., n/2; block b of the stage with h = n/(2t) blocks uses table[h + b];
+//   x' = (x + y) / 2, y' = (x - y) w (mod Q)                                       (src/amx_kernels.cpp:461-498)
+//   v = inter + acc, inter = (scan sum * Q + 2^31) >> 32; rescale to q1; OR the q1_bits-bit values LSB-first into
+//   the prefix from bit row1_off                                                   (src/amx_kernels.cpp:306, 515-537)
+// The stages run in rounds of three (bits s0..s0+2 of the coefficient index): in a round a thread holds the 8
+// coefficients that differ only in those bits, so three stages need one shared-memory exchange.  Coefficient i is
+// stored at word i ^ (8 * ((i >> 6) & 3)), which keeps every round's accesses free of bank conflicts.
+__device__ __forceinline__ int tail_swz(int i) { return i ^ (((i >> 6) & 3) << 3); }
+
+template <int L>
+__device__ __forceinline__ int tail_index(int o, int m, int s0, int r) {
+  return ((o >> s0) << (s0 + r)) | (m << s0) | (o & ((1 << s0) - 1));
+}
+
+// Three (or fewer) stages on the 2^r coefficients x[0..2^r) of one group, whose index is i(m) = tail_index(o, m).
+template <int L>
+__device__ __forceinline__ void tail_round(uint32_t *x, int o, int s0, int r, const uint32_t *__restrict__ tw) {
+  constexpr int n = 1 << L;
+  for (int d = 0; d < r; ++d) {
+    const int s = s0 + d, t = 1 << d;
+    for (int m = 0; m < (1 << r); ++m) {
+      if (m & t) continue;
+      const int i = tail_index<L>(o, m, s0, r);
+      const uint32_t w = __ldg(tw + (n >> (s + 1)) + (i >> (s + 1)));
+      const uint32_t a = x[m], b = x[m + t];
+      x[m] = half_q(add_q(a, b));
+      x[m + t] = mul_q(sub_q(a, b), w);
+    }
+  }
+}
+
+template <int L>
+__global__ void __launch_bounds__((1 << L) / 8) tail_kernel(TailArgs a) {
+  constexpr int n = 1 << L, NT = n / 8;
   extern __shared__ uint32_t tsm[];
   const int slot = blockIdx.x / a.outputs, o = blockIdx.x % a.outputs;
   if (a.status[slot] != 0) return;  // rejected frames get no response (their output stays untouched)
-  const int n = a.n, tid = threadIdx.x, nt = blockDim.x;
+  const int tid = threadIdx.x;
   uint32_t *acc = tsm;
   uint32_t *res = tsm + n;
   const int res_words = (a.part_len + 3) / 4 + 1;
@@ -128,44 +138,136 @@ __global__ void __launch_bounds__(256) tail_kernel(TailArgs a) {
   const uint32_t *th = a.that + (size_t)o * count;
   const size_t base = (size_t)slot * a.cols + (size_t)o * n;
 
+  // prefix -> res (32-bit words, little endian)
+  const uint8_t *pre = a.prefix + (size_t)o * a.part_len;
+  if ((a.part_len & 15) == 0 && (reinterpret_cast<uintptr_t>(pre) & 15) == 0) {
+    for (int w = tid; w < a.part_len / 16; w += NT) {
+      const uint4 v = *reinterpret_cast<const uint4 *>(pre + 16 * w);
+      res[4 * w] = v.x; res[4 * w + 1] = v.y; res[4 * w + 2] = v.z; res[4 * w + 3] = v.w;
+    }
+    if (tid == 0) res[a.part_len / 4] = 0;
+  } else {
+    for (int w = tid; w < res_words; w += NT) {
+      uint32_t v = 0;
+      for (int b = 0; b < 4; ++b)
+        if (4 * w + b < a.part_len) v |= (uint32_t)pre[4 * w + b] << (8 * b);
+      res[w] = v;
+    }
+  }
+
+  // key-switch accumulate for coefficients 8 tid .. 8 tid + 7, then stages t = 1, 2, 4 in registers
+  uint32_t x[8];
+  {
+    const int i0 = 8 * tid;
+    const uint4 b0 = *reinterpret_cast<const uint4 *>(a.beta + base + i0);
+    const uint4 b1 = *reinterpret_cast<const uint4 *>(a.beta + base + i0 + 4);
+    x[0] = b0.x; x[1] = b0.y; x[2] = b0.z; x[3] = b0.w; x[4] = b1.x; x[5] = b1.y; x[6] = b1.z; x[7] = b1.w;
+    for (int k = 0; k < a.tg; ++k) {
+      const uint4 z0 = *reinterpret_cast<const uint4 *>(z + (size_t)k * n + i0);
+      const uint4 z1 = *reinterpret_cast<const uint4 *>(z + (size_t)k * n + i0 + 4);
+      const uint4 t0 = *reinterpret_cast<const uint4 *>(th + (size_t)k * n + i0);
+      const uint4 t1 = *reinterpret_cast<const uint4 *>(th + (size_t)k * n + i0 + 4);
+      x[0] = add_q(x[0], mul_q(z0.x, t0.x)); x[1] = add_q(x[1], mul_q(z0.y, t0.y));
+      x[2] = add_q(x[2], mul_q(z0.z, t0.z)); x[3] = add_q(x[3], mul_q(z0.w, t0.w));
+      x[4] = add_q(x[4], mul_q(z1.x, t1.x)); x[5] = add_q(x[5], mul_q(z1.y, t1.y));
+      x[6] = add_q(x[6], mul_q(z1.z, t1.z)); x[7] = add_q(x[7], mul_q(z1.w, t1.w));
+    }
+    tail_round<L>(x, tid, 0, 3, a.twiddle);
+  }
+
+  // rounds over bits 3..5, 6..8, ...: exchange through shared memory, three stages per round
+#pragma unroll
+  for (int s0 = 3; s0 < L; s0 += 3) {
+    const int r = (L - s0) < 3 ? (L - s0) : 3;
+    const int groups = 8 >> r;
+    const int ps0 = s0 - 3, pr = 3;  // the previous round's layout (every round but the last has three bits)
+    // write the 8 values held from the previous round
+    if (s0 == 3) {
+      // coefficients 8 tid .. 8 tid + 7 stay contiguous under the swizzle (it only flips bits 3 and 4)
+      uint4 *dst4 = reinterpret_cast<uint4 *>(acc + tail_swz(8 * tid));
+      dst4[0] = make_uint4(x[0], x[1], x[2], x[3]);
+      dst4[1] = make_uint4(x[4], x[5], x[6], x[7]);
+    } else {
+#pragma unroll
+      for (int m = 0; m < 8; ++m) acc[tail_swz(tail_index<L>(tid, m, ps0, pr))] = x[m];
+    }
+    __syncthreads();
+    for (int g = 0; g < groups; ++g) {
+      const int oo = g * NT + tid;
+      uint32_t y[8];
+      for (int m = 0; m < (1 << r); ++m) y[m] = acc[tail_swz(tail_index<L>(oo, m, s0, r))];
+      tail_round<L>(y, oo, s0, r, a.twiddle);
+      if (s0 + r < L) {
+        for (int m = 0; m < 8; ++m) x[m] = y[m];
+      } else {
+        // last round: modulus switch of these coefficients and their bits into the response part
+        for (int m = 0; m < (1 << r); ++m) {
+          const int i = tail_index<L>(oo, m, s0, r);
+          const uint32_t inter = (uint32_t)(((uint64_t)a.acc[base + i] * kQ + (1ull << 31)) >> 32);
+          const uint32_t t = rescale_q(add_q(inter, y[m]), (uint32_t)a.q1);
+          const uint32_t p = (uint32_t)a.row1_off + (uint32_t)i * (uint32_t)a.q1_bits;
+          const uint32_t sh = p & 31u;
+          atomicOr(&res[p >> 5], t << sh);
+          if (sh) {
+            const uint32_t hi = t >> (32u - sh);
+            if (hi) atomicOr(&res[(p >> 5) + 1], hi);
+          }
+        }
+      }
+    }
+    if (s0 + r < L) __syncthreads();
+  }
+  __syncthreads();
+
+  uint8_t *dst = a.resp + (size_t)slot * a.resp_stride + (size_t)o * a.part_len;
+  if ((a.part_len & 15) == 0 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+    for (int w = tid; w < a.part_len / 16; w += NT)
+      *reinterpret_cast<uint4 *>(dst + 16 * w) = make_uint4(res[4 * w], res[4 * w + 1], res[4 * w + 2], res[4 * w + 3]);
+  } else {
+    for (int b = tid; b < a.part_len; b += NT) dst[b] = (uint8_t)(res[b >> 2] >> (8 * (b & 3)));
+  }
+}
+
+// The same computation for small rings (n < 256), one coefficient pair per thread and stage.
+__global__ void __launch_bounds__(128) tail_small_kernel(TailArgs a) {
+  extern __shared__ uint32_t tsm[];
+  const int slot = blockIdx.x / a.outputs, o = blockIdx.x % a.outputs;
+  if (a.status[slot] != 0) return;
+  const int n = a.n, tid = threadIdx.x, nt = blockDim.x;
+  uint32_t *acc = tsm;
+  uint32_t *res = tsm + n;
+  const int res_words = (a.part_len + 3) / 4 + 1;
+  const size_t count = (size_t)a.tg * n;
+  const uint32_t *z = reinterpret_cast<const uint32_t *>(a.req + (size_t)slot * a.req_stride + a.z_off);
+  const uint32_t *th = a.that + (size_t)o * count;
+  const size_t base = (size_t)slot * a.cols + (size_t)o * n;
   for (int i = tid; i < n; i += nt) {
     uint32_t s = a.beta[base + i];
-    for (int k = 0; k < a.tg; ++k) s = addmod_q(s, mulmod_q(z[(size_t)k * n + i], th[(size_t)k * n + i]));
+    for (int k = 0; k < a.tg; ++k) s = add_q(s, mul_q(z[(size_t)k * n + i], th[(size_t)k * n + i]));
     acc[i] = s;
   }
   const uint8_t *pre = a.prefix + (size_t)o * a.part_len;
   for (int w = tid; w < res_words; w += nt) {
     uint32_t v = 0;
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int idx = 4 * w + b;
-      if (idx < a.part_len) v |= (uint32_t)pre[idx] << (8 * b);
-    }
+    for (int b = 0; b < 4; ++b)
+      if (4 * w + b < a.part_len) v |= (uint32_t)pre[4 * w + b] << (8 * b);
     res[w] = v;
   }
   __syncthreads();
-
-  for (int t = 1; t < n; t <<= 1) {
-    const int h = n / (2 * t);
+  for (int lt = 0; (1 << lt) < n; ++lt) {
+    const int t = 1 << lt, h = n >> (lt + 1);
     for (int b = tid; b < n / 2; b += nt) {
-      const int blk = b / t, j = b - blk * t;
+      const int blk = b >> lt, j = b & (t - 1);
       const int i0 = 2 * t * blk + j, i1 = i0 + t;
-      const uint32_t x = acc[i0], y = acc[i1], w = a.twiddle[h + blk];
-      uint64_t s = (uint64_t)x + y;
-      if (s >= kQ) s -= kQ;
-      s = (s & 1) ? (s + kQ) >> 1 : s >> 1;
-      uint64_t d = (uint64_t)x + kQ - y;
-      if (d >= kQ) d -= kQ;
-      acc[i0] = (uint32_t)s;
-      acc[i1] = mulmod_q((uint32_t)d, w);
+      const uint32_t x = acc[i0], y = acc[i1];
+      acc[i0] = half_q(add_q(x, y));
+      acc[i1] = mul_q(sub_q(x, y), a.twiddle[h + blk]);
     }
     __syncthreads();
   }
-
   for (int i = tid; i < n; i += nt) {
     const uint32_t inter = (uint32_t)(((uint64_t)a.acc[base + i] * kQ + (1ull << 31)) >> 32);
-    const uint32_t v = addmod_q(inter, acc[i]);
-    const uint32_t t = rescale_q1(v, a.q1);
+    const uint32_t t = rescale_q(add_q(inter, acc[i]), (uint32_t)a.q1);
     const uint32_t p = (uint32_t)a.row1_off + (uint32_t)i * (uint32_t)a.q1_bits;
     const uint32_t sh = p & 31u;
     atomicOr(&res[p >> 5], t << sh);
@@ -175,14 +277,8 @@ __global__ void __launch_bounds__(256) tail_kernel(TailArgs a) {
     }
   }
   __syncthreads();
-
   uint8_t *dst = a.resp + (size_t)slot * a.resp_stride + (size_t)o * a.part_len;
-  if ((a.part_len & 3) == 0 && ((reinterpret_cast<uintptr_t>(dst) & 3) == 0)) {
-    uint32_t *d32 = reinterpret_cast<uint32_t *>(dst);
-    for (int w = tid; w < a.part_len / 4; w += nt) d32[w] = res[w];
-  } else {
-    for (int b = tid; b < a.part_len; b += nt) dst[b] = (uint8_t)(res[b >> 2] >> (8 * (b & 3)));
-  }
+  for (int b = tid; b < a.part_len; b += nt) dst[b] = (uint8_t)(res[b >> 2] >> (8 * (b & 3)));
 }
 
 // ------------------------------------------------------------------------------------ synthetic database
@@ -208,6 +304,33 @@ __global__ void synthetic_db_kernel(uint8_t *db, size_t ld, size_t rows, size_t 
     word |= ((col & 1) ? (v >> 8) : (v & 0xff)) << (8 * b);
   }
   *reinterpret_cast<uint32_t *>(db + c * ld + r0) = word;
+}
+
+}  // namespace alto
+
+namespace alto {
+
+// Launches the tail for `slots` frames on stream st: the radix-8 kernel for n >= 256, the simple one below.
+inline cudaError_t launch_tail(const TailArgs &t, size_t slots, cudaStream_t st) {
+  const size_t smem = ((size_t)t.n + (t.part_len + 3) / 4 + 1) * sizeof(uint32_t);
+  const unsigned grid = (unsigned)(slots * t.outputs);
+  cudaError_t err = cudaSuccess;
+  auto go = [&](auto kernel, unsigned threads) {
+    if (smem > 48 * 1024) err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err == cudaSuccess) {
+      kernel<<<grid, threads, smem, st>>>(t);
+      err = cudaGetLastError();
+    }
+  };
+  switch (t.n) {
+    case 256: go(tail_kernel<8>, 32); break;
+    case 512: go(tail_kernel<9>, 64); break;
+    case 1024: go(tail_kernel<10>, 128); break;
+    case 2048: go(tail_kernel<11>, 256); break;
+    case 4096: go(tail_kernel<12>, 512); break;
+    default: go(tail_small_kernel, 128); break;
+  }
+  return err;
 }
 
 }  // namespace alto

@@ -1,0 +1,69 @@
+// modq.cuh -- exact arithmetic modulo Q = 4294955009 = 2^32 - 12287 on 32-bit residues, shared by host and device.
+//
+// All inputs are residues in [0, Q) unless stated.  Q > 2^31, so sums overflow 32 bits; the helpers use the wrap of
+// unsigned arithmetic, which subtracts 2^32 = Q + 12287, to stay in 32-bit registers.
+#pragma once
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define ALTO_HD __host__ __device__ __forceinline__
+#else
+#define ALTO_HD inline
+#endif
+
+namespace alto {
+
+constexpr uint32_t kQ32 = 4294955009u;
+constexpr uint32_t kFold = 12287u;  // 2^32 mod Q
+
+// (a + b) mod Q.  On a carry the true sum a + b = s + 2^32 >= Q, and s - Q (mod 2^32) = s + 12287 is that sum
+// minus Q; without a carry one conditional subtraction suffices.
+ALTO_HD uint32_t add_q(uint32_t a, uint32_t b) {
+  const uint32_t s = a + b;
+  return (s < a || s >= kQ32) ? s - kQ32 : s;
+}
+
+// (a - b) mod Q.
+ALTO_HD uint32_t sub_q(uint32_t a, uint32_t b) {
+  const uint32_t d = a - b;
+  return a < b ? d + kQ32 : d;
+}
+
+// s / 2 mod Q (Q odd): s / 2 when s is even, (s + Q) / 2 = (s >> 1) + (Q + 1) / 2 when s is odd.
+ALTO_HD uint32_t half_q(uint32_t s) { return (s >> 1) + ((s & 1u) ? (kQ32 + 1u) / 2u : 0u); }
+
+// x mod Q for any 64-bit x: x = h 2^32 + l = 12287 h + l (mod Q); two folds leave x < 2^32 + 2^28.
+ALTO_HD uint32_t red_q64(uint64_t x) {
+  x = (x >> 32) * kFold + (x & 0xffffffffull);
+  x = (x >> 32) * kFold + (x & 0xffffffffull);
+  return (uint32_t)(x >= kQ32 ? x - kQ32 : x);
+}
+
+// (a * b) mod Q for any 32-bit a, b.
+ALTO_HD uint32_t mul_q(uint32_t a, uint32_t b) { return red_q64((uint64_t)a * b); }
+
+// floor(u / Q) for u < 2^53.  u / 2^32 <= u / Q, so q0 = u >> 32 undershoots; the remainder u - q0 Q =
+// (u mod 2^32) + 12287 q0 < 2^32 + 2^35 leaves at most a few more multiples of Q, found the same way.
+ALTO_HD uint64_t div_q(uint64_t u) {
+  const uint64_t q0 = u >> 32;
+  uint64_t r = (u & 0xffffffffull) + q0 * kFold;
+  const uint64_t q1 = r >> 32;
+  r = (r & 0xffffffffull) + q1 * kFold;
+  return q0 + q1 + (r >= kQ32 ? 1u : 0u);
+}
+
+// Centred rescale of v in [0, Q) from Q to q1 (q1 < 2^21), rounding half away from zero, result in [0, q1):
+// c = v or v - Q (centred), t = trunc((c q1 +- floor(Q/2)) / Q), t + q1 when negative, t - q1 when t = q1
+// (src/amx_kernels.cpp:522-529; the reference divides in double precision, which rounds to the same integer).
+ALTO_HD uint32_t rescale_q(uint32_t v, uint32_t q1) {
+  constexpr uint64_t half = kQ32 / 2u;
+  const bool neg = v >= (uint32_t)half;
+  const uint64_t mag = neg ? (uint64_t)(kQ32 - v) : (uint64_t)v;  // |c|
+  const uint64_t t = div_q(mag * q1 + half);                       // |trunc(x / Q)|, same sign as c
+  int64_t s = neg ? -(int64_t)t : (int64_t)t;
+  if (s < 0) s += q1;
+  if (s >= (int64_t)q1) s -= q1;
+  return (uint32_t)s;
+}
+
+}  // namespace alto

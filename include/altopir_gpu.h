@@ -73,7 +73,8 @@ size_t alto_response_len(const void *engine);
  *   != tg * n, 3 for a y or z key word >= q, else 0 (query words are not range-checked);
  *   out[c] (alto_response_len bytes) is written for status 0 only, other output buffers stay untouched.
  * method must be 0 (the reference's AMX code) or 2 (VNNI); both run the same GPU path.  When stage_ms is not NULL
- * it receives device times in ms of [0] upload + validation, [1] limb split + scan, [2] pack, [3] tail + download.
+ * it receives device times in ms of the reference's four stages: [0] key upload + validation, [1] scan (including
+ * any wait for the query upload, which overlaps the pack), [2] pack, [3] tail + download.
  * Returns the number of valid requests, -1 for bad arguments, -3 when the tail parameters are invalid (n not a
  * power of two >= 16, q1 >= 2^21, q1_bits > 24, n % 8, or row 1 not fitting in part_len), -4 when the device
  * failed (CUDA error or a kernel wait that timed out; alto_last_error() has the reason).  Calls on one engine must
@@ -147,6 +148,10 @@ void alto_fill_uniform_u64(uint64_t *dst, size_t count, uint64_t bound, uint64_t
 void alto_fill_bytes(uint8_t *dst, size_t count, uint64_t seed, int threads);
 void alto_synthetic_request(uint8_t *frame, size_t rows, size_t tg_n, uint64_t seed, uint64_t client);
 void alto_pack_encode(int8_t *ub, const uint32_t *U, size_t cols, size_t K, int threads);
+
+/* Self-check of the engine's modulus-switch arithmetic on the host: sum over v in [v0, v1) of rescale(v) * (2v + 1)
+ * modulo 2^64, where rescale is the exact integer centred rescale Q -> q1 that the tail kernel runs. */
+uint64_t alto_rescale_digest(uint64_t q1, uint64_t v0, uint64_t v1, int threads);
 
 #ifdef __cplusplus
 }

@@ -173,6 +173,15 @@ uint64_t orc_rescale_mismatches(uint64_t v0, uint64_t v1, uint64_t q1) {
     return bad;
 }
 
+/* Position-weighted digest of orc_rescale over [v0, v1): sum of rescale(v) * (2v + 1) mod 2^64, to compare a
+ * whole range with another implementation in one number. */
+uint64_t orc_rescale_digest(uint64_t v0, uint64_t v1, uint64_t q1) {
+    uint64_t d = 0;
+    #pragma omp parallel for reduction(+ : d) schedule(static)
+    for (int64_t v = (int64_t)v0; v < (int64_t)v1; v++) d += (uint64_t)orc_rescale((uint64_t)v, q1) * (2 * (uint64_t)v + 1);
+    return d;
+}
+
 /* Row 1 of one response part (amx_kernels.cpp:515-537): rescale inter + acc and OR q1_bits-bit values LSB-first into
  * res at bit bit_off + z * q1_bits, never past res_len.  Returns -1 on the reference's parameter check. */
 int orc_switch_row1(uint8_t *res, size_t res_len, size_t bit_off, const uint32_t *inter, const uint64_t *acc, size_t n,

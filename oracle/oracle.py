@@ -88,6 +88,7 @@ class Oracle:
             ("orc_rescale", U32, [U64, U64]),
             ("orc_rescale_double", U32, [U64, U64]),
             ("orc_rescale_mismatches", U64, [U64, U64, U64]),
+            ("orc_rescale_digest", U64, [U64, U64, U64]),
             ("orc_switch_row1", I, [P, S, S, P, P, S, U64, I]),
             ("orc_tail_ntt", I, [P, P, P, P, S, P, S]),
             ("orc_answer_part", I, [c.POINTER(_OrcState), P, S, P]),
@@ -146,6 +147,9 @@ class Oracle:
 
     def rescale_mismatches(self, v0, v1, q1):
         return self.L.orc_rescale_mismatches(v0, v1, q1)
+
+    def rescale_digest(self, v0, v1, q1):
+        return self.L.orc_rescale_digest(v0, v1, q1)
 
     def rescale(self, v, q1):
         return self.L.orc_rescale(v, q1)

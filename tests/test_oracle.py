@@ -107,6 +107,18 @@ def test_oracle_rescale_integer_equals_double_exhaustively(oracle):
             assert oracle.rescale_mismatches(v0, min(v0 + 200000, Q), q1) == 0
 
 
+def test_engine_rescale_arithmetic_matches_oracle_exhaustively(oracle):
+    # the tail kernel's division-free rescale (modq.cuh, compiled for the host here) against the oracle's plain
+    # integer division, over every v in [0, Q) for q1 = 2^10 and strided ranges for other q1 < 2^21
+    import altopir_b200 as pkg
+    L = pkg.lib()
+    Q = 4294955009
+    assert L.alto_rescale_digest(1 << 10, 0, Q, 0) == oracle.rescale_digest(0, Q, 1 << 10)
+    for q1 in (1, 3, 1000, (1 << 20) + 7, (1 << 21) - 1):
+        for v0 in (0, Q // 2 - 100000, Q - 200000):
+            assert L.alto_rescale_digest(q1, v0, v0 + 200000, 0) == oracle.rescale_digest(v0, v0 + 200000, q1)
+
+
 def test_synthetic_record_three_ways(oracle, svc):
     for row in (0, 1, 977, 2047, 123456):
         a = svc.synthetic_record(row, 4096)
