@@ -16,6 +16,7 @@
 
 #include "../../include/altopir_gpu.h"
 #include "kernels.cuh"
+#include "limb_gemm2.cuh"
 
 namespace {
 
@@ -230,6 +231,53 @@ bool dispatch_gemm(int bn, const CUtensorMap &a, const CUtensorMap &b, const alt
   return false;
 }
 
+template <int BN, alto::Epi EPI>
+bool launch_pair(const CUtensorMap &a, const CUtensorMap &b, const alto::PairArgs &g, int pairs, cudaStream_t st) {
+  const int smem = alto::PairShape<BN>::kSmemBytes;
+  ALTO_CK(cudaFuncSetAttribute(alto::limb_gemm_pair_kernel<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               smem));
+  alto::limb_gemm_pair_kernel<BN, EPI><<<2 * pairs, alto::kGemmThreads, smem, st>>>(a, b, g);
+  ALTO_CK(cudaGetLastError());
+  return true;
+}
+
+template <alto::Epi EPI>
+bool dispatch_pair(int bn, const CUtensorMap &a, const CUtensorMap &b, const alto::PairArgs &g, int pairs,
+                   cudaStream_t st) {
+  switch (bn) {
+    case 32: return launch_pair<32, EPI>(a, b, g, pairs, st);
+    case 64: return launch_pair<64, EPI>(a, b, g, pairs, st);
+    case 128: return launch_pair<128, EPI>(a, b, g, pairs, st);
+    case 256: return launch_pair<256, EPI>(a, b, g, pairs, st);
+  }
+  set_error("unsupported pair GEMM tile width");
+  return false;
+}
+
+// CTA pairs that can be resident at once (clusters of two CTAs, one CTA per SM); 74 on a 148-SM B200.
+int resident_pairs() {
+  static int cached = 0;
+  if (!cached) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(sms & ~1);
+    cfg.blockDim = dim3(alto::kGemmThreads);
+    cfg.dynamicSmemBytes = alto::PairShape<256>::kSmemBytes;
+    int clusters = 0;
+    cudaFuncSetAttribute(alto::limb_gemm_pair_kernel<256, alto::Epi::kScan>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, alto::PairShape<256>::kSmemBytes);
+    if (cudaOccupancyMaxActiveClusters(&clusters, alto::limb_gemm_pair_kernel<256, alto::Epi::kScan>, &cfg) !=
+            cudaSuccess ||
+        clusters <= 0)
+      clusters = sms / 2;
+    cudaGetLastError();
+    cached = clusters;
+  }
+  return cached;
+}
+
 int pick_bn(size_t limb_cols) {
   for (int bn : {16, 32, 64, 128})
     if (limb_cols <= (size_t)bn) return bn;
@@ -237,29 +285,125 @@ int pick_bn(size_t limb_cols) {
 }
 
 struct Plan {
+  bool pair = false;  // CTA-pair kernels (limb columns > 16) or the single-CTA kernels
   int bn = 16, num_n = 1;
   int scan_m = 0, scan_split = 1, scan_kb_per = 1, scan_kb = 0;
   int pack_m = 0, pack_kb = 0;
+  int pairs_scan = 0, pairs_pack = 0;  // persistent grid of the pair kernels
 };
+
+// ALTO_GEMM=single forces the single-CTA kernels (a tuning override; both compute identical results).
+bool pair_kernels_enabled() {
+  const char *v = getenv("ALTO_GEMM");
+  return !(v && strcmp(v, "single") == 0);
+}
 
 Plan make_plan(const Engine *e, size_t slots) {
   Plan p;
   const size_t limb_cols = 4 * round_up(slots, 4);
-  p.bn = pick_bn(limb_cols);
-  p.num_n = (int)((limb_cols + p.bn - 1) / p.bn);
-  p.scan_m = (int)((e->cols + alto::kBM - 1) / alto::kBM);
+  p.pair = limb_cols > 16 && pair_kernels_enabled();
   p.scan_kb = (int)((e->rows + alto::kBK - 1) / alto::kBK);
-  // Split the record axis so that (a) no chunk exceeds 256 blocks = 32768 records, which bounds every int32 limb
-  // partial sum by 32768 * 255 * 255 < 2^31, and (b) there are about four units per SM, each at least 8 blocks long.
+  p.pack_kb = (int)(e->count / alto::kBK);
+  if (!p.pair) {
+    p.bn = pick_bn(limb_cols);
+    p.num_n = (int)((limb_cols + p.bn - 1) / p.bn);
+    p.scan_m = (int)((e->cols + alto::kBM - 1) / alto::kBM);
+    p.pack_m = (int)((4 * e->cols + alto::kBM - 1) / alto::kBM);
+    // Split the record axis so that (a) no chunk exceeds 256 blocks = 32768 records, which bounds every int32 limb
+    // partial sum by 32768 * 255 * 255 < 2^31, and (b) there are about four units per SM, each >= 8 blocks long.
+    const long tiles = (long)p.scan_m * p.num_n;
+    long split = std::max<long>((p.scan_kb + 255) / 256, (4L * 148 + tiles - 1) / tiles);
+    split = std::min<long>(split, std::max<long>(1, p.scan_kb / 8));
+    split = std::max<long>(split, (p.scan_kb + 255) / 256);
+    p.scan_kb_per = (int)((p.scan_kb + split - 1) / split);
+    p.scan_split = (p.scan_kb + p.scan_kb_per - 1) / p.scan_kb_per;
+    return p;
+  }
+  p.bn = 32;
+  while (p.bn < 256 && (size_t)p.bn < limb_cols) p.bn *= 2;
+  p.num_n = (int)((limb_cols + p.bn - 1) / p.bn);
+  p.scan_m = (int)((e->cols + 255) / 256);
+  p.pack_m = (int)((4 * e->cols + 255) / 256);
+  const int pairs = resident_pairs();
+  // Scan chunks: at most 256 blocks (exactness, as above), at least 8, and about twelve units per resident pair so
+  // the persistent pairs finish together.
   const long tiles = (long)p.scan_m * p.num_n;
-  long split = std::max<long>((p.scan_kb + 255) / 256, (4L * 148 + tiles - 1) / tiles);
+  long split = std::max<long>((p.scan_kb + 255) / 256, (12L * pairs + tiles - 1) / tiles);
   split = std::min<long>(split, std::max<long>(1, p.scan_kb / 8));
   split = std::max<long>(split, (p.scan_kb + 255) / 256);
   p.scan_kb_per = (int)((p.scan_kb + split - 1) / split);
   p.scan_split = (p.scan_kb + p.scan_kb_per - 1) / p.scan_kb_per;
-  p.pack_m = (int)((4 * e->cols + alto::kBM - 1) / alto::kBM);
-  p.pack_kb = (int)(e->count / alto::kBK);
+  p.pairs_scan = (int)std::min<long>(pairs, tiles * p.scan_split);
+  p.pairs_pack = (int)std::min<long>(pairs, (long)p.pack_m * p.num_n);
   return p;
+}
+
+// The scan GEMM (acc sums, pre-zeroed) and the pack GEMM (beta) for `slots` clients under plan p.
+bool launch_scan(const Engine *e, const Plan &p, const CUtensorMap &map_q, uint32_t *acc, size_t slots,
+                 cudaStream_t st) {
+  if (p.pair) {
+    alto::PairArgs g;
+    g.num_m = p.scan_m;
+    g.num_n = p.num_n;
+    g.num_units = p.scan_m * p.num_n * p.scan_split;
+    g.kb_total = p.scan_kb;
+    g.kb_per_unit = p.scan_kb_per;
+    g.rows_a = (int)e->cols;
+    g.clients = (int)slots;
+    g.cols = (int)e->cols;
+    g.out = acc;
+    g.err = e->d_err;
+    return dispatch_pair<alto::Epi::kScan>(p.bn, e->map_db, map_q, g, p.pairs_scan, st);
+  }
+  alto::GemmArgs g;
+  g.num_m = p.scan_m;
+  g.num_n = p.num_n;
+  g.kb_total = p.scan_kb;
+  g.kb_per_unit = p.scan_kb_per;
+  g.rows_a = (int)e->cols;
+  g.clients = (int)slots;
+  g.cols = (int)e->cols;
+  g.out = acc;
+  g.err = e->d_err;
+  return dispatch_gemm<alto::Epi::kScan>(p.bn, e->map_db, map_q, g, p.scan_m * p.num_n * p.scan_split, st);
+}
+
+bool launch_pack(const Engine *e, const Plan &p, const CUtensorMap &map_y, uint32_t *beta, size_t slots,
+                 cudaStream_t st) {
+  if (p.pair) {
+    alto::PairArgs g;
+    g.num_m = p.pack_m;
+    g.num_n = p.num_n;
+    g.num_units = p.pack_m * p.num_n;
+    g.kb_total = p.pack_kb;
+    g.kb_per_unit = p.pack_kb;
+    g.rows_a = (int)(4 * e->cols);
+    g.clients = (int)slots;
+    g.cols = (int)e->cols;
+    g.out = beta;
+    g.err = e->d_err;
+    return dispatch_pair<alto::Epi::kPack>(p.bn, e->map_ub, map_y, g, p.pairs_pack, st);
+  }
+  alto::GemmArgs g;
+  g.num_m = p.pack_m;
+  g.num_n = p.num_n;
+  g.kb_total = p.pack_kb;
+  g.kb_per_unit = p.pack_kb;
+  g.rows_a = (int)(4 * e->cols);
+  g.clients = (int)slots;
+  g.cols = (int)e->cols;
+  g.out = beta;
+  g.err = e->d_err;
+  return dispatch_gemm<alto::Epi::kPack>(p.bn, e->map_ub, map_y, g, p.pack_m * p.num_n, st);
+}
+
+// Tensor maps of the two limb operands for plan p (B boxes are BN rows for the single-CTA kernels and BN/2 rows,
+// one half per CTA, for the pair kernels).
+bool make_limb_maps(const Engine *e, const Plan &p, const uint8_t *qlimb, const uint8_t *ylimb, size_t bp,
+                    CUtensorMap *map_q, CUtensorMap *map_y) {
+  const uint32_t box = (uint32_t)(p.pair ? p.bn / 2 : p.bn);
+  return make_map(map_q, qlimb, e->rows, 4 * (uint64_t)bp, e->rows, box) &&
+         make_map(map_y, ylimb, e->count, 4 * (uint64_t)bp, e->count, box);
 }
 
 // Enqueues the answer path for `slots` staged frames on the engine's stream: validate, key limb split, pack GEMM,
@@ -287,8 +431,7 @@ bool enqueue_batch(Engine *e, const uint8_t *d_slots, size_t slot_stride, size_t
   ALTO_CK(cudaEventRecord(mk[1], st));
 
   CUtensorMap map_q, map_y;
-  if (!make_map(&map_q, e->d_qlimb, e->rows, 4 * (uint64_t)bp, e->rows, (uint32_t)p.bn)) return false;
-  if (!make_map(&map_y, e->d_ylimb, e->count, 4 * (uint64_t)bp, e->count, (uint32_t)p.bn)) return false;
+  if (!make_limb_maps(e, p, e->d_qlimb, e->d_ylimb, bp, &map_q, &map_y)) return false;
   const unsigned split_threads = 256;
   {
     const size_t work = (e->count / 16) * (size_t)bp;
@@ -298,20 +441,8 @@ bool enqueue_batch(Engine *e, const uint8_t *d_slots, size_t slot_stride, size_t
     ALTO_CK(cudaGetLastError());
   }
   ALTO_CK(cudaEventRecord(mk[2], st));
-  {
-    alto::GemmArgs g;
-    g.num_m = p.pack_m;
-    g.num_n = p.num_n;
-    g.kb_total = p.pack_kb;
-    g.kb_per_unit = p.pack_kb;
-    g.rows_a = (int)(4 * e->cols);
-    g.clients = (int)slots;
-    g.cols = (int)e->cols;
-    g.out = e->d_beta;
-    g.err = e->d_err;
-    if (!dispatch_gemm<alto::Epi::kPack>(p.bn, e->map_ub, map_y, g, p.pack_m * p.num_n, st)) return false;
-    ++launches;
-  }
+  if (!launch_pack(e, p, map_y, e->d_beta, slots, st)) return false;
+  ++launches;
   ALTO_CK(cudaEventRecord(mk[3], st));
   if (queries_ready) ALTO_CK(cudaStreamWaitEvent(st, queries_ready, 0));
   {
@@ -323,21 +454,8 @@ bool enqueue_batch(Engine *e, const uint8_t *d_slots, size_t slot_stride, size_t
   }
   ALTO_CK(cudaMemsetAsync(e->d_acc, 0, slots * e->cols * sizeof(uint32_t), st));
   ALTO_CK(cudaEventRecord(mk[4], st));
-  {
-    alto::GemmArgs g;
-    g.num_m = p.scan_m;
-    g.num_n = p.num_n;
-    g.kb_total = p.scan_kb;
-    g.kb_per_unit = p.scan_kb_per;
-    g.rows_a = (int)e->cols;
-    g.clients = (int)slots;
-    g.cols = (int)e->cols;
-    g.out = e->d_acc;
-    g.err = e->d_err;
-    if (!dispatch_gemm<alto::Epi::kScan>(p.bn, e->map_db, map_q, g, p.scan_m * p.num_n * p.scan_split, st))
-      return false;
-    ++launches;
-  }
+  if (!launch_scan(e, p, map_q, e->d_acc, slots, st)) return false;
+  ++launches;
   ALTO_CK(cudaEventRecord(mk[5], st));
   {
     alto::TailArgs t;
@@ -798,25 +916,9 @@ bool enqueue_noalloc(Engine *e, uint8_t *scratch, const NoAllocLayout &l, const 
       d_slots, stride, kSlotLead + 9, (int)b, bp, e->count, ylimb);
   ALTO_CK(cudaGetLastError());
   CUtensorMap map_q, map_y;
-  if (!make_map(&map_q, qlimb, e->rows, 4 * (uint64_t)bp, e->rows, (uint32_t)p.bn)) return false;
-  if (!make_map(&map_y, ylimb, e->count, 4 * (uint64_t)bp, e->count, (uint32_t)p.bn)) return false;
-  alto::GemmArgs g;
-  g.num_m = p.scan_m;
-  g.num_n = p.num_n;
-  g.kb_total = p.scan_kb;
-  g.kb_per_unit = p.scan_kb_per;
-  g.rows_a = (int)e->cols;
-  g.clients = (int)b;
-  g.cols = (int)e->cols;
-  g.out = acc;
-  g.err = e->d_err;
-  if (!dispatch_gemm<alto::Epi::kScan>(p.bn, e->map_db, map_q, g, p.scan_m * p.num_n * p.scan_split, st)) return false;
-  g.num_m = p.pack_m;
-  g.kb_total = p.pack_kb;
-  g.kb_per_unit = p.pack_kb;
-  g.rows_a = (int)(4 * e->cols);
-  g.out = beta;
-  if (!dispatch_gemm<alto::Epi::kPack>(p.bn, e->map_ub, map_y, g, p.pack_m * p.num_n, st)) return false;
+  if (!make_limb_maps(e, p, qlimb, ylimb, bp, &map_q, &map_y)) return false;
+  if (!launch_scan(e, p, map_q, acc, b, st)) return false;
+  if (!launch_pack(e, p, map_y, beta, b, st)) return false;
   alto::TailArgs t;
   t.acc = acc;
   t.beta = beta;
