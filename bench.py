@@ -138,7 +138,11 @@ def int8_cublas_tops(torch):
         return None
 
 
-def traffic_from_profile(kernel):
+def traffic_from_profile(kernel, rows, record_bytes, batch):
+    """DRAM bytes per launch of `kernel` from the committed ncu capture (profiles/ncu_traffic.json), which covers the
+    default workload only; None for any other configuration."""
+    if (rows, record_bytes, batch) != (32768, 32768, 128):
+        return None
     path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     try:
         with open(path) as f:
@@ -346,7 +350,7 @@ def main_ours(a):
     kernels["validate"] = {"avg_ms": kms[0] / max(nb, 1)}
     kernels["limb_split"] = {"avg_ms": kms[1] / max(nb, 1)}
     kernels["tail"] = {"avg_ms": kms[4] / max(nb, 1)}
-    traffic = traffic_from_profile(dom)
+    traffic = traffic_from_profile(dom, a.rows, a.record_bytes, B)
     roofline = {"kernel": dom, "bound": "tensor", "achieved": kernels[dom]["tops"], "peak": int8_peak,
                 "unit": "TFLOP/s", "frac": kernels[dom]["tops"] / int8_peak, "traffic": traffic,
                 "peak_source": f"2 x {peak_src} dense bf16 ({peaks['bf16_tflops']} TF/s; B200 int8 dense rate = 2x "
