@@ -80,10 +80,16 @@ class Engine:
             raise EngineError(f"unsupported engine configuration: {last_error()}")
 
     @staticmethod
-    def from_state(st, threads=1):
-        """Prepared::engine (src/service.rs:159-170) for a service.SyntheticState."""
+    def from_state(st, threads=1, tile=True):
+        """Prepared::engine (src/service.rs:159-170) for a service.SyntheticState.  With tile=False no tiled copy
+        is made (this engine reads the column-order database and never the tiled one), which halves the host
+        memory of very large databases."""
         p = st.p
-        tiled = TiledDb(st.db_col, st.db_col.shape[1], p.rows, p.record_bytes, threads)
+        if tile:
+            tiled = TiledDb(st.db_col, st.db_col.shape[1], p.rows, p.record_bytes, threads)
+        else:
+            tiled = TiledDb.__new__(TiledDb)
+            tiled.rows, tiled.cols, tiled.buf = p.rows, p.record_bytes, np.zeros(64, dtype=np.uint8)
         return Engine(st.db_col, tiled, st.db_col.shape[1], st.ub, p.n, p.tg, st.prefixes, p.row1_off, 1 << p.q1_bits,
                       p.q1_bits, st.that, st.inv_table, Q, threads)
 

@@ -262,6 +262,16 @@ int orc_answer(const OrcState *s, const uint8_t *const *req, const size_t *len, 
     return bad ? -3 : (int)valid;
 }
 
+/* A list of response parts computed in parallel: part k is output parts[k] of the (valid) frame frames[k], written
+ * to out[k] (part_len bytes each).  Returns -3 if any tail failed. */
+int orc_answer_parts(const OrcState *s, const uint8_t *const *frames, const size_t *parts, size_t count,
+                     uint8_t *const *out) {
+    int bad = 0;
+    #pragma omp parallel for schedule(dynamic, 1) reduction(| : bad)
+    for (size_t k = 0; k < count; k++) bad |= orc_answer_part(s, frames[k], parts[k], out[k]) != 0;
+    return bad ? -3 : 0;
+}
+
 /* ---------------------------------------------------------------- packing matrix (amx_kernels.cpp:311-341) */
 
 /* The dense public packing matrix with the InspiRING automorphisms folded in, as values mod Q:

@@ -94,6 +94,7 @@ class Oracle:
             ("orc_answer_part", I, [c.POINTER(_OrcState), P, S, P]),
             ("orc_answer", I, [c.POINTER(_OrcState), c.POINTER(P), c.POINTER(S), S, c.POINTER(P), c.POINTER(I)]),
             ("orc_pack_build", None, [P, c.POINTER(P), c.POINTER(P), P, P, S, S, S, S]),
+            ("orc_answer_parts", I, [c.POINTER(_OrcState), c.POINTER(P), c.POINTER(S), S, c.POINTER(P)]),
         ]:
             f = getattr(L, name)
             f.restype, f.argtypes = res, args
@@ -139,6 +140,19 @@ class Oracle:
         if r:
             raise RuntimeError(f"oracle tail failure {r}")
         return res
+
+    def answer_parts(self, st, frames, parts):
+        """Output part parts[k] of frame frames[k] for every k, computed in parallel; returns a (k, part_len) array."""
+        s, keep = self._state(st)
+        k = len(frames)
+        out = np.zeros((k, st.prefixes[0].size), dtype=np.uint8)
+        fp = (ctypes.c_void_p * k)(*[f.ctypes.data for f in frames])
+        pp = (ctypes.c_size_t * k)(*[int(x) for x in parts])
+        op = (ctypes.c_void_p * k)(*[out[i].ctypes.data for i in range(k)])
+        r = self.L.orc_answer_parts(ctypes.byref(s), fp, pp, k, op)
+        if r:
+            raise RuntimeError(f"oracle tail failure {r}")
+        return out
 
     def validate(self, frame, count, rows):
         if frame is None:
