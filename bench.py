@@ -237,7 +237,8 @@ def main_ours(a):
     p = svc.params(a.rows, a.record_bytes)
     want_cpu = rank == 0 and world == 1 and not a.no_cpu_baseline
     st = svc.SyntheticState.make(p, seed=1, keep_values=want_cpu)
-    e = eng.Engine.from_state(st, threads=svc.threads())
+    # the engine reads the column-order database; skip the host tiled copy of very large databases
+    e = eng.Engine.from_state(st, threads=svc.threads(), tile=a.rows * a.record_bytes <= (8 << 30))
     if not want_cpu:
         st.ub = None
     B, rl, ql = a.batch, e.response_len(), e.request_len()
