@@ -82,7 +82,37 @@ bool make_map(CUtensorMap *m, const void *base, uint64_t inner, uint64_t outer, 
   return true;
 }
 
+// The scan operands as 3-D maps: `outer` record chunks of `mid` rows x `inner` bytes (row stride `inner`, chunk
+// stride mid * inner), read in boxes of 128 bytes x box_rows rows of one chunk.
+bool make_map3(CUtensorMap *m, const void *base, uint64_t inner, uint64_t mid, uint64_t outer, uint32_t box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) {
+    set_error("cuTensorMapEncodeTiled is unavailable");
+    return false;
+  }
+  const cuuint64_t dims[3] = {inner, mid, outer};
+  const cuuint64_t strides[2] = {inner, inner * mid};
+  const cuuint32_t box[3] = {128, box_rows, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void *>(base), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "cuTensorMapEncodeTiled failed (%d) for %llu x %llu x %llu, box rows %u", (int)r,
+             (unsigned long long)outer, (unsigned long long)mid, (unsigned long long)inner, box_rows);
+    set_error(buf);
+    return false;
+  }
+  return true;
+}
+
 size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Records per chunk of the scan operands in HBM.  A database column of R records would otherwise put every column
+// of a 128-column TMA box on its own page once R reaches ~2^20 (the TLB then misses on every box); chunks of 32768
+// records keep a box inside a few pages.  32768 is also the longest reduction an int32 limb sum can take exactly.
+constexpr size_t kRecordChunk = 32768;
 
 // ------------------------------------------------------------------------------------------- engine
 struct Engine {
@@ -90,6 +120,7 @@ struct Engine {
   cudaStream_t st = nullptr;
   size_t rows = 0, cols = 0, n = 0, tg = 0, outputs = 0, count = 0, part_len = 0, row1_off = 0, want = 0;
   size_t resp_len = 0, slot_stride = 0;
+  size_t chunk = 0, nchunks = 1;  // record chunking of the database and the query limbs
   uint64_t q1 = 0;
   int q1_bits = 0, threads = 1;
   bool tail_ok = false;
@@ -196,7 +227,7 @@ bool ensure_capacity(Engine *e, size_t slots) {
   free_scratch(e);
   const size_t cap = round_up(slots, 4);
   ALTO_CK(cudaMalloc(&e->d_req, cap * e->slot_stride));
-  ALTO_CK(cudaMalloc(&e->d_qlimb, 4 * cap * e->rows));
+  ALTO_CK(cudaMalloc(&e->d_qlimb, 4 * cap * e->chunk * e->nchunks));
   ALTO_CK(cudaMalloc(&e->d_ylimb, 4 * cap * e->count));
   ALTO_CK(cudaMalloc(&e->d_resp, cap * e->resp_len));
   ALTO_CK(cudaMalloc(&e->d_status, cap * sizeof(int)));
@@ -286,6 +317,7 @@ int pick_bn(size_t limb_cols) {
 
 struct Plan {
   bool pair = false;  // CTA-pair kernels (limb columns > 16) or the single-CTA kernels
+  int kb_chunk = 1;   // scan blocks per record chunk
   int bn = 16, num_n = 1;
   int scan_m = 0, scan_split = 1, scan_kb_per = 1, scan_kb = 0;
   int pack_m = 0, pack_kb = 0;
@@ -304,6 +336,14 @@ Plan make_plan(const Engine *e, size_t slots) {
   p.pair = limb_cols > 16 && pair_kernels_enabled();
   p.scan_kb = (int)((e->rows + alto::kBK - 1) / alto::kBK);
   p.pack_kb = (int)(e->count / alto::kBK);
+  // with several record chunks a unit must stay inside one: its length divides the 256 blocks of a chunk
+  p.kb_chunk = e->nchunks > 1 ? (int)(e->chunk / alto::kBK) : std::max(p.scan_kb, 1);
+  auto chunk_aligned = [&](int kb_per) {
+    if (e->nchunks == 1) return kb_per;
+    int d = p.kb_chunk;
+    while (d / 2 >= kb_per && d % 2 == 0) d /= 2;
+    return d;  // the smallest divisor of a chunk's blocks (a power of two here) that is >= kb_per
+  };
   if (!p.pair) {
     p.bn = pick_bn(limb_cols);
     p.num_n = (int)((limb_cols + p.bn - 1) / p.bn);
@@ -315,7 +355,7 @@ Plan make_plan(const Engine *e, size_t slots) {
     long split = std::max<long>((p.scan_kb + 255) / 256, (4L * 148 + tiles - 1) / tiles);
     split = std::min<long>(split, std::max<long>(1, p.scan_kb / 8));
     split = std::max<long>(split, (p.scan_kb + 255) / 256);
-    p.scan_kb_per = (int)((p.scan_kb + split - 1) / split);
+    p.scan_kb_per = chunk_aligned((int)((p.scan_kb + split - 1) / split));
     p.scan_split = (p.scan_kb + p.scan_kb_per - 1) / p.scan_kb_per;
     return p;
   }
@@ -331,7 +371,7 @@ Plan make_plan(const Engine *e, size_t slots) {
   long split = std::max<long>((p.scan_kb + 255) / 256, (12L * pairs + tiles - 1) / tiles);
   split = std::min<long>(split, std::max<long>(1, p.scan_kb / 8));
   split = std::max<long>(split, (p.scan_kb + 255) / 256);
-  p.scan_kb_per = (int)((p.scan_kb + split - 1) / split);
+  p.scan_kb_per = chunk_aligned((int)((p.scan_kb + split - 1) / split));
   p.scan_split = (p.scan_kb + p.scan_kb_per - 1) / p.scan_kb_per;
   p.pairs_scan = (int)std::min<long>(pairs, tiles * p.scan_split);
   p.pairs_pack = (int)std::min<long>(pairs, (long)p.pack_m * p.num_n);
@@ -341,6 +381,9 @@ Plan make_plan(const Engine *e, size_t slots) {
 // The scan GEMM (acc sums, pre-zeroed) and the pack GEMM (beta) for `slots` clients under plan p.
 bool launch_scan(const Engine *e, const Plan &p, const CUtensorMap &map_q, uint32_t *acc, size_t slots,
                  cudaStream_t st) {
+  // The query limbs are re-read by every unit of a K chunk; mark them evict-last only while the whole operand
+  // (4 bytes per record and client) is a small part of the 126 MB L2, so stale chunks never crowd it out.
+  const int keep_b = 4 * round_up(slots, 4) * e->rows <= (size_t(32) << 20);
   if (p.pair) {
     alto::PairArgs g;
     g.num_m = p.scan_m;
@@ -353,6 +396,8 @@ bool launch_scan(const Engine *e, const Plan &p, const CUtensorMap &map_q, uint3
     g.cols = (int)e->cols;
     g.out = acc;
     g.err = e->d_err;
+    g.b_keep = keep_b;
+    g.kb_chunk = p.kb_chunk;
     return dispatch_pair<alto::Epi::kScan>(p.bn, e->map_db, map_q, g, p.pairs_scan, st);
   }
   alto::GemmArgs g;
@@ -365,11 +410,14 @@ bool launch_scan(const Engine *e, const Plan &p, const CUtensorMap &map_q, uint3
   g.cols = (int)e->cols;
   g.out = acc;
   g.err = e->d_err;
+  g.b_keep = keep_b;
+  g.kb_chunk = p.kb_chunk;
   return dispatch_gemm<alto::Epi::kScan>(p.bn, e->map_db, map_q, g, p.scan_m * p.num_n * p.scan_split, st);
 }
 
 bool launch_pack(const Engine *e, const Plan &p, const CUtensorMap &map_y, uint32_t *beta, size_t slots,
                  cudaStream_t st) {
+  const int keep_b = 4 * round_up(slots, 4) * e->count <= (size_t(32) << 20);
   if (p.pair) {
     alto::PairArgs g;
     g.num_m = p.pack_m;
@@ -382,6 +430,8 @@ bool launch_pack(const Engine *e, const Plan &p, const CUtensorMap &map_y, uint3
     g.cols = (int)e->cols;
     g.out = beta;
     g.err = e->d_err;
+    g.b_keep = keep_b;
+    g.kb_chunk = 1;
     return dispatch_pair<alto::Epi::kPack>(p.bn, e->map_ub, map_y, g, p.pairs_pack, st);
   }
   alto::GemmArgs g;
@@ -394,6 +444,8 @@ bool launch_pack(const Engine *e, const Plan &p, const CUtensorMap &map_y, uint3
   g.cols = (int)e->cols;
   g.out = beta;
   g.err = e->d_err;
+  g.b_keep = keep_b;
+  g.kb_chunk = 1;
   return dispatch_gemm<alto::Epi::kPack>(p.bn, e->map_ub, map_y, g, p.pack_m * p.num_n, st);
 }
 
@@ -402,7 +454,7 @@ bool launch_pack(const Engine *e, const Plan &p, const CUtensorMap &map_y, uint3
 bool make_limb_maps(const Engine *e, const Plan &p, const uint8_t *qlimb, const uint8_t *ylimb, size_t bp,
                     CUtensorMap *map_q, CUtensorMap *map_y) {
   const uint32_t box = (uint32_t)(p.pair ? p.bn / 2 : p.bn);
-  return make_map(map_q, qlimb, e->rows, 4 * (uint64_t)bp, e->rows, box) &&
+  return make_map3(map_q, qlimb, e->chunk, 4 * (uint64_t)bp, e->nchunks, box) &&
          make_map(map_y, ylimb, e->count, 4 * (uint64_t)bp, e->count, box);
 }
 
@@ -436,7 +488,7 @@ bool enqueue_batch(Engine *e, const uint8_t *d_slots, size_t slot_stride, size_t
   {
     const size_t work = (e->count / 16) * (size_t)bp;
     alto::limb_split_kernel<<<(unsigned)((work + split_threads - 1) / split_threads), split_threads, 0, st>>>(
-        d_slots, slot_stride, kSlotLead + 9, (int)slots, bp, e->count, e->d_ylimb);
+        d_slots, slot_stride, kSlotLead + 9, (int)slots, bp, e->count, e->count, e->d_ylimb);
     ++launches;
     ALTO_CK(cudaGetLastError());
   }
@@ -448,7 +500,7 @@ bool enqueue_batch(Engine *e, const uint8_t *d_slots, size_t slot_stride, size_t
   {
     const size_t work = (e->rows / 16) * (size_t)bp;
     alto::limb_split_kernel<<<(unsigned)((work + split_threads - 1) / split_threads), split_threads, 0, st>>>(
-        d_slots, slot_stride, kSlotLead + 9 + 8 * e->count, (int)slots, bp, e->rows, e->d_qlimb);
+        d_slots, slot_stride, kSlotLead + 9 + 8 * e->count, (int)slots, bp, e->rows, e->chunk, e->d_qlimb);
     ++launches;
     ALTO_CK(cudaGetLastError());
   }
@@ -693,9 +745,19 @@ void *alto_engine_new(const uint8_t *db_col, const uint8_t *db_tiled, size_t ld,
   for (auto &set : e->marks)
     for (cudaEvent_t &ev : set)
       if ((err = cudaEventCreate(&ev)) != cudaSuccess) return fail("event", err);
-  if ((err = cudaMalloc(&e->d_db, rows * cols)) != cudaSuccess) return fail("database", err);
-  if ((err = cudaMemcpy2D(e->d_db, rows, db_col, ld, rows, cols, cudaMemcpyHostToDevice)) != cudaSuccess)
-    return fail("database upload", err);
+  e->chunk = rows > kRecordChunk ? kRecordChunk : rows;
+  e->nchunks = (rows + e->chunk - 1) / e->chunk;
+  // database in HBM as [chunk][col][record in chunk]; the tail of a partial last chunk is zero
+  if ((err = cudaMalloc(&e->d_db, e->nchunks * e->chunk * cols)) != cudaSuccess) return fail("database", err);
+  if (rows % e->chunk &&
+      (err = cudaMemset(e->d_db + (e->nchunks - 1) * e->chunk * cols, 0, e->chunk * cols)) != cudaSuccess)
+    return fail("database padding", err);
+  for (size_t z = 0; z < e->nchunks; ++z) {
+    const size_t r0 = z * e->chunk, nr = std::min(e->chunk, rows - r0);
+    if ((err = cudaMemcpy2D(e->d_db + z * e->chunk * cols, e->chunk, db_col + r0, ld, nr, cols,
+                            cudaMemcpyHostToDevice)) != cudaSuccess)
+      return fail("database upload", err);
+  }
   if ((err = cudaMalloc(&e->d_ub, 4 * e->count * cols)) != cudaSuccess) return fail("packing matrix", err);
   if ((err = cudaMemcpy(e->d_ub, ub, 4 * e->count * cols, cudaMemcpyHostToDevice)) != cudaSuccess)
     return fail("packing matrix upload", err);
@@ -721,7 +783,7 @@ void *alto_engine_new(const uint8_t *db_col, const uint8_t *db_tiled, size_t ld,
   if ((err = cudaMemset(e->d_err, 0, sizeof(uint32_t))) != cudaSuccess) return fail("error word", err);
   if ((err = cudaHostAlloc(&e->h_err, sizeof(uint32_t), cudaHostAllocDefault)) != cudaSuccess)
     return fail("pinned error word", err);
-  if (!make_map(&e->map_db, e->d_db, rows, cols, rows, alto::kBM) ||
+  if (!make_map3(&e->map_db, e->d_db, e->chunk, cols, e->nchunks, alto::kBM) ||
       !make_map(&e->map_ub, e->d_ub, e->count, 4 * cols, e->count, alto::kBM)) {
     destroy(e);
     return nullptr;
@@ -881,7 +943,7 @@ NoAllocLayout noalloc_layout(const Engine *e, size_t b) {
   l.status = off;
   off = round_up(off + b * sizeof(int), 256);
   l.qlimb = off;
-  off = round_up(off + 4 * bp * e->rows, 256);
+  off = round_up(off + 4 * bp * e->chunk * e->nchunks, 256);
   l.ylimb = off;
   off = round_up(off + 4 * bp * e->count, 256);
   l.acc = off;
@@ -908,12 +970,12 @@ bool enqueue_noalloc(Engine *e, uint8_t *scratch, const NoAllocLayout &l, const 
   ALTO_CK(cudaGetLastError());
   const size_t qwork = (e->rows / 16) * (size_t)bp;
   alto::limb_split_kernel<<<(unsigned)((qwork + split_threads - 1) / split_threads), split_threads, 0, st>>>(
-      d_slots, stride, kSlotLead + 9 + 8 * e->count, (int)b, bp, e->rows, qlimb);
+      d_slots, stride, kSlotLead + 9 + 8 * e->count, (int)b, bp, e->rows, e->chunk, qlimb);
   ALTO_CK(cudaGetLastError());
   ALTO_CK(cudaMemsetAsync(acc, 0, b * e->cols * sizeof(uint32_t), st));  // the scan adds into these sums
   const size_t ywork = (e->count / 16) * (size_t)bp;
   alto::limb_split_kernel<<<(unsigned)((ywork + split_threads - 1) / split_threads), split_threads, 0, st>>>(
-      d_slots, stride, kSlotLead + 9, (int)b, bp, e->count, ylimb);
+      d_slots, stride, kSlotLead + 9, (int)b, bp, e->count, e->count, ylimb);
   ALTO_CK(cudaGetLastError());
   CUtensorMap map_q, map_y;
   if (!make_limb_maps(e, p, qlimb, ylimb, bp, &map_q, &map_y)) return false;

@@ -33,10 +33,11 @@ __global__ void validate_kernel(const uint8_t *__restrict__ slots, size_t stride
 }
 
 // ------------------------------------------------------------------------------------ limb split
-// dst[(c * 4 + j) * words + k] = byte j of word k of slot c, for c < padded (zero rows for c >= slots).  This is
-// the K-major B operand of the limb GEMMs.  Each thread moves 16 words (64 bytes in, four 16-byte rows out).
+// Byte j of word k of slot c goes to dst[z][(c * 4 + j)][k - z * chunk] with z = k / chunk, for c < padded (zero
+// rows for c >= slots): the K-major B operand of the limb GEMMs, cut into record chunks of `chunk` words (a
+// multiple of 16) like the database.  Each thread moves 16 words (64 bytes in, four 16-byte rows out).
 __global__ void limb_split_kernel(const uint8_t *__restrict__ req, size_t stride, size_t word_off, int slots,
-                                  int padded, size_t words, uint8_t *__restrict__ dst) {
+                                  int padded, size_t words, size_t chunk, uint8_t *__restrict__ dst) {
   const size_t groups = words / 16;
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= groups * (size_t)padded) return;
@@ -67,9 +68,11 @@ __global__ void limb_split_kernel(const uint8_t *__restrict__ req, size_t stride
 #pragma unroll
       for (int q = 0; q < 4; ++q) o[j][q] = 0;
   }
+  const size_t k = g * 16, z = k / chunk;
+  uint8_t *base = dst + z * (4 * (size_t)padded * chunk) + (k - z * chunk);
 #pragma unroll
   for (int j = 0; j < 4; ++j)
-    *reinterpret_cast<uint4 *>(dst + ((size_t)c * 4 + j) * words + g * 16) = make_uint4(o[j][0], o[j][1], o[j][2], o[j][3]);
+    *reinterpret_cast<uint4 *>(base + ((size_t)c * 4 + j) * chunk) = make_uint4(o[j][0], o[j][1], o[j][2], o[j][3]);
 }
 
 // ------------------------------------------------------------------------------------ tail

@@ -35,6 +35,8 @@ struct GemmArgs {
   int cols;         // record bytes: row stride of the output matrices
   uint32_t *out;    // scan: acc[c * cols + col], pre-zeroed; pack: beta[c * cols + col]
   uint32_t *err;    // device error word
+  int b_keep;       // 1: keep the B operand in L2 (evict_last; it is small and read by every unit), 0: normal
+  int kb_chunk;     // scan: 128-byte blocks per record chunk of the 3-D operand maps (units never straddle chunks)
 };
 
 // x mod Q for any 64-bit x, using 2^32 = 12287 (mod Q): two folds leave x < 2^32 + 2^28, one subtraction finishes.
@@ -111,15 +113,23 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     // ---------------------------------------------------------------- TMA producer
     if (lane == 0) {
       // The A operand (database or packing matrix) streams through once per unit; B (limbs) is shared by all units.
-      const uint64_t pol_a = policy_evict_first(), pol_b = policy_evict_last();
+      const uint64_t pol_a = policy_evict_first();
+      const uint64_t pol_b = args.b_keep ? policy_evict_last() : policy_evict_normal();
       int issued = 0;
       for (int i = 0; i < nkb; ++i) {
         const int s = i % kStages, round = i / kStages;
         if (round > 0 && !mbar_wait(empty0 + 8 * s, (round - 1) & 1, args.err, ALTO_ERR_WAIT_EMPTY, bail)) break;
         const uint32_t sa = base_addr + s * S::kStageBytes, sb = sa + S::kABytes;
         mbar_arrive_expect_tx(full0 + 8 * s, S::kStageBytes);
-        tma_load_2d(sa, &map_a, full0 + 8 * s, (kb0 + i) * kBK, m_tile * kBM, pol_a);
-        tma_load_2d(sb, &map_b, full0 + 8 * s, (kb0 + i) * kBK, n_tile * BN, pol_b);
+        if constexpr (EPI == Epi::kScan) {
+          // record chunk z, 128-byte block x inside it
+          const int kb = kb0 + i, z = kb / args.kb_chunk, x = (kb - z * args.kb_chunk) * kBK;
+          tma_load_3d(sa, &map_a, full0 + 8 * s, x, m_tile * kBM, z, pol_a);
+          tma_load_3d(sb, &map_b, full0 + 8 * s, x, n_tile * BN, z, pol_b);
+        } else {
+          tma_load_2d(sa, &map_a, full0 + 8 * s, (kb0 + i) * kBK, m_tile * kBM, pol_a);
+          tma_load_2d(sb, &map_b, full0 + 8 * s, (kb0 + i) * kBK, n_tile * BN, pol_b);
+        }
         issued = i + 1;
       }
       if (*bail) {

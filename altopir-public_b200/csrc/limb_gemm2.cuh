@@ -45,6 +45,8 @@ struct PairArgs {
   int cols;         // record bytes: row stride of the outputs
   uint32_t *out;    // scan: acc[c * cols + col] (pre-zeroed, summed mod 2^32); pack: beta[c * cols + col]
   uint32_t *err;    // device error word
+  int b_keep;       // 1: keep the B operand in L2 (evict_last; it is small and read by every unit), 0: normal
+  int kb_chunk;     // scan: 128-byte blocks per record chunk of the 3-D operand maps (units never straddle chunks)
 };
 
 // Epilogue of 16 TMEM columns (4 clients x 4 limbs) for one accumulator row of the scan: row = database column.
@@ -138,7 +140,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
   if (warp == 0) {
     // ------------------------------------------------------------ TMA producer (both CTAs)
     if (lane == 0) {
-      const uint64_t pol_a = policy_evict_first(), pol_b = policy_evict_last();
+      const uint64_t pol_a = policy_evict_first();
+      const uint64_t pol_b = args.b_keep ? policy_evict_last() : policy_evict_normal();
       const uint32_t full_leader0 = map_to_rank(full0, 0);
       int g = 0;
       bool stop = false;
@@ -153,9 +156,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
           }
           const uint32_t sa = base_addr + s * S::kStageBytes, sb = sa + S::kABytes;
           if (leader) mbar_arrive_expect_tx(full0 + 8 * s, 2 * S::kStageBytes);
-          const int x = (kb0 + i) * kBK;
-          tma_load_2d_pair(sa, &map_a, full_leader0 + 8 * s, x, m * 256 + (int)rank * 128, pol_a);
-          tma_load_2d_pair(sb, &map_b, full_leader0 + 8 * s, x, n * BN + (int)rank * (BN / 2), pol_b);
+          if constexpr (EPI == Epi::kScan) {
+            const int kb = kb0 + i, z = kb / args.kb_chunk, x = (kb - z * args.kb_chunk) * kBK;
+            tma_load_3d_pair(sa, &map_a, full_leader0 + 8 * s, x, m * 256 + (int)rank * 128, z, pol_a);
+            tma_load_3d_pair(sb, &map_b, full_leader0 + 8 * s, x, n * BN + (int)rank * (BN / 2), z, pol_b);
+          } else {
+            const int x = (kb0 + i) * kBK;
+            tma_load_2d_pair(sa, &map_a, full_leader0 + 8 * s, x, m * 256 + (int)rank * 128, pol_a);
+            tma_load_2d_pair(sb, &map_b, full_leader0 + 8 * s, x, n * BN + (int)rank * (BN / 2), pol_b);
+          }
         }
       }
       if (stop) {
