@@ -9,7 +9,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libaltopir_gpu.so")
 SOURCES = ["csrc/alto_engine.cu", "csrc/host_setup.cpp"]
-DEPS = SOURCES + ["csrc/kernels.cuh", "csrc/limb_gemm.cuh", "csrc/sm100.cuh", "../include/altopir_gpu.h"]
+DEPS = SOURCES + ["csrc/kernels.cuh", "csrc/limb_gemm.cuh", "csrc/limb_gemm2.cuh", "csrc/sm100.cuh", "csrc/modq.cuh",
+                  "csrc/serving.cuh", "../include/altopir_gpu.h"]
 
 
 def nvcc_path():

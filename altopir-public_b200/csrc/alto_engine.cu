@@ -115,9 +115,21 @@ size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 constexpr size_t kRecordChunk = 32768;
 
 // ------------------------------------------------------------------------------------------- engine
+// The device resources of one batch in flight: its stream, per-batch scratch (grown on demand) and error word.
+// An engine answers through its `main` batch; a serving loop keeps several so that batches overlap on the device.
+struct Batch {
+  cudaStream_t st = nullptr;
+  size_t cap = 0;
+  uint8_t *d_req = nullptr, *d_qlimb = nullptr, *d_ylimb = nullptr, *d_resp = nullptr;
+  int *d_status = nullptr;
+  uint32_t *d_acc = nullptr, *d_beta = nullptr;
+  int *h_status = nullptr;
+  uint32_t *d_err = nullptr, *h_err = nullptr;
+  bool timing = false;  // record per-kernel timing marks into the engine's ring (main batch only)
+};
+
 struct Engine {
   int dev = -1;
-  cudaStream_t st = nullptr;
   size_t rows = 0, cols = 0, n = 0, tg = 0, outputs = 0, count = 0, part_len = 0, row1_off = 0, want = 0;
   size_t resp_len = 0, slot_stride = 0;
   size_t chunk = 0, nchunks = 1;  // record chunking of the database and the query limbs
@@ -126,14 +138,8 @@ struct Engine {
   bool tail_ok = false;
   // resident state
   uint8_t *d_db = nullptr, *d_ub = nullptr, *d_prefix = nullptr;
-  uint32_t *d_that = nullptr, *d_tw = nullptr, *d_err = nullptr;
-  // per-batch scratch, grown on demand
-  size_t cap = 0;
-  uint8_t *d_req = nullptr, *d_qlimb = nullptr, *d_ylimb = nullptr, *d_resp = nullptr;
-  int *d_status = nullptr;
-  uint32_t *d_acc = nullptr, *d_beta = nullptr;
-  int *h_status = nullptr;
-  uint32_t *h_err = nullptr;
+  uint32_t *d_that = nullptr, *d_tw = nullptr;
+  Batch main;
   // per call: before the uploads, after the downloads; the query words upload on st_copy
   cudaEvent_t ev_begin = nullptr, ev_end = nullptr, ev_keys = nullptr, ev_queries = nullptr;
   cudaStream_t st_copy = nullptr;
@@ -182,34 +188,51 @@ bool next_set(Engine *e, int *set) {
   return true;
 }
 
-void free_scratch(Engine *e) {
-  cudaFree(e->d_req);
-  cudaFree(e->d_qlimb);
-  cudaFree(e->d_ylimb);
-  cudaFree(e->d_resp);
-  cudaFree(e->d_status);
-  cudaFree(e->d_acc);
-  cudaFree(e->d_beta);
-  cudaFreeHost(e->h_status);
-  e->d_req = e->d_qlimb = e->d_ylimb = e->d_resp = nullptr;
-  e->d_status = nullptr;
-  e->d_acc = e->d_beta = nullptr;
-  e->h_status = nullptr;
-  e->cap = 0;
+void free_scratch(Batch *b) {
+  cudaFree(b->d_req);
+  cudaFree(b->d_qlimb);
+  cudaFree(b->d_ylimb);
+  cudaFree(b->d_resp);
+  cudaFree(b->d_status);
+  cudaFree(b->d_acc);
+  cudaFree(b->d_beta);
+  cudaFreeHost(b->h_status);
+  b->d_req = b->d_qlimb = b->d_ylimb = b->d_resp = nullptr;
+  b->d_status = nullptr;
+  b->d_acc = b->d_beta = nullptr;
+  b->h_status = nullptr;
+  b->cap = 0;
+}
+
+// Stream, error word and its pinned mirror of a batch (scratch comes later, on demand).
+bool init_batch(Batch *b, bool timing) {
+  ALTO_CK(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
+  ALTO_CK(cudaMalloc(&b->d_err, sizeof(uint32_t)));
+  ALTO_CK(cudaMemset(b->d_err, 0, sizeof(uint32_t)));
+  ALTO_CK(cudaHostAlloc(&b->h_err, sizeof(uint32_t), cudaHostAllocDefault));
+  b->timing = timing;
+  return true;
+}
+
+void destroy_batch(Batch *b) {
+  if (b->st) cudaStreamSynchronize(b->st);
+  free_scratch(b);
+  cudaFree(b->d_err);
+  cudaFreeHost(b->h_err);
+  if (b->st) cudaStreamDestroy(b->st);
+  b->st = nullptr;
+  b->d_err = b->h_err = nullptr;
 }
 
 void destroy(Engine *e) {
   if (!e) return;
   if (e->dev >= 0) cudaSetDevice(e->dev);
-  if (e->st) cudaStreamSynchronize(e->st);
-  free_scratch(e);
+  if (e->main.st) cudaStreamSynchronize(e->main.st);
   cudaFree(e->d_db);
   cudaFree(e->d_ub);
   cudaFree(e->d_prefix);
   cudaFree(e->d_that);
   cudaFree(e->d_tw);
-  cudaFree(e->d_err);
-  cudaFreeHost(e->h_err);
   if (e->st_copy) cudaStreamSynchronize(e->st_copy);
   for (cudaEvent_t ev : {e->ev_begin, e->ev_end, e->ev_keys, e->ev_queries})
     if (ev) cudaEventDestroy(ev);
@@ -217,24 +240,24 @@ void destroy(Engine *e) {
   for (auto &set : e->marks)
     for (cudaEvent_t &ev : set)
       if (ev) cudaEventDestroy(ev);
-  if (e->st) cudaStreamDestroy(e->st);
+  destroy_batch(&e->main);
   delete e;
 }
 
-bool ensure_capacity(Engine *e, size_t slots) {
-  if (slots <= e->cap) return true;
-  ALTO_CK(cudaStreamSynchronize(e->st));
-  free_scratch(e);
+bool ensure_capacity(const Engine *e, Batch *b, size_t slots) {
+  if (slots <= b->cap) return true;
+  ALTO_CK(cudaStreamSynchronize(b->st));
+  free_scratch(b);
   const size_t cap = round_up(slots, 4);
-  ALTO_CK(cudaMalloc(&e->d_req, cap * e->slot_stride));
-  ALTO_CK(cudaMalloc(&e->d_qlimb, 4 * cap * e->chunk * e->nchunks));
-  ALTO_CK(cudaMalloc(&e->d_ylimb, 4 * cap * e->count));
-  ALTO_CK(cudaMalloc(&e->d_resp, cap * e->resp_len));
-  ALTO_CK(cudaMalloc(&e->d_status, cap * sizeof(int)));
-  ALTO_CK(cudaMalloc(&e->d_acc, cap * e->cols * sizeof(uint32_t)));
-  ALTO_CK(cudaMalloc(&e->d_beta, cap * e->cols * sizeof(uint32_t)));
-  ALTO_CK(cudaHostAlloc(&e->h_status, cap * sizeof(int), cudaHostAllocDefault));
-  e->cap = cap;
+  ALTO_CK(cudaMalloc(&b->d_req, cap * e->slot_stride));
+  ALTO_CK(cudaMalloc(&b->d_qlimb, 4 * cap * e->chunk * e->nchunks));
+  ALTO_CK(cudaMalloc(&b->d_ylimb, 4 * cap * e->count));
+  ALTO_CK(cudaMalloc(&b->d_resp, cap * e->resp_len));
+  ALTO_CK(cudaMalloc(&b->d_status, cap * sizeof(int)));
+  ALTO_CK(cudaMalloc(&b->d_acc, cap * e->cols * sizeof(uint32_t)));
+  ALTO_CK(cudaMalloc(&b->d_beta, cap * e->cols * sizeof(uint32_t)));
+  ALTO_CK(cudaHostAlloc(&b->h_status, cap * sizeof(int), cudaHostAllocDefault));
+  b->cap = cap;
   return true;
 }
 
@@ -262,19 +285,25 @@ bool dispatch_gemm(int bn, const CUtensorMap &a, const CUtensorMap &b, const alt
   return false;
 }
 
-template <int BN, alto::Epi EPI>
+template <int BN, alto::Epi EPI, int NSUB = 1>
 bool launch_pair(const CUtensorMap &a, const CUtensorMap &b, const alto::PairArgs &g, int pairs, cudaStream_t st) {
-  const int smem = alto::PairShape<BN>::kSmemBytes;
-  ALTO_CK(cudaFuncSetAttribute(alto::limb_gemm_pair_kernel<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               smem));
-  alto::limb_gemm_pair_kernel<BN, EPI><<<2 * pairs, alto::kGemmThreads, smem, st>>>(a, b, g);
+  const int smem = alto::PairShape<BN, NSUB>::kSmemBytes;
+  ALTO_CK(cudaFuncSetAttribute(alto::limb_gemm_pair_kernel<BN, EPI, NSUB>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  alto::limb_gemm_pair_kernel<BN, EPI, NSUB><<<2 * pairs, alto::kGemmThreads, smem, st>>>(a, b, g);
   ALTO_CK(cudaGetLastError());
   return true;
 }
 
+// bn = columns per accumulator; wide = two 256-column accumulators per unit (NSUB = 2, scan only)
 template <alto::Epi EPI>
 bool dispatch_pair(int bn, const CUtensorMap &a, const CUtensorMap &b, const alto::PairArgs &g, int pairs,
-                   cudaStream_t st) {
+                   cudaStream_t st, bool wide = false) {
+  if (wide) {
+    if (bn == 256) return launch_pair<256, EPI, 2>(a, b, g, pairs, st);
+    set_error("wide pair GEMM needs 256-column accumulators");
+    return false;
+  }
   switch (bn) {
     case 32: return launch_pair<32, EPI>(a, b, g, pairs, st);
     case 64: return launch_pair<64, EPI>(a, b, g, pairs, st);
@@ -286,27 +315,29 @@ bool dispatch_pair(int bn, const CUtensorMap &a, const CUtensorMap &b, const alt
 }
 
 // CTA pairs that can be resident at once (clusters of two CTAs, one CTA per SM); 74 on a 148-SM B200.
+int compute_resident_pairs() {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(sms & ~1);
+  cfg.blockDim = dim3(alto::kGemmThreads);
+  cfg.dynamicSmemBytes = alto::PairShape<256>::kSmemBytes;
+  int clusters = 0;
+  cudaFuncSetAttribute(alto::limb_gemm_pair_kernel<256, alto::Epi::kScan>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       alto::PairShape<256>::kSmemBytes);
+  if (cudaOccupancyMaxActiveClusters(&clusters, alto::limb_gemm_pair_kernel<256, alto::Epi::kScan>, &cfg) !=
+          cudaSuccess ||
+      clusters <= 0)
+    clusters = sms / 2;
+  cudaGetLastError();
+  return clusters;
+}
+
+// CTA pairs that can be resident at once (clusters of two CTAs, one CTA per SM); 74 on a 148-SM B200.
 int resident_pairs() {
-  static int cached = 0;
-  if (!cached) {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(sms & ~1);
-    cfg.blockDim = dim3(alto::kGemmThreads);
-    cfg.dynamicSmemBytes = alto::PairShape<256>::kSmemBytes;
-    int clusters = 0;
-    cudaFuncSetAttribute(alto::limb_gemm_pair_kernel<256, alto::Epi::kScan>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, alto::PairShape<256>::kSmemBytes);
-    if (cudaOccupancyMaxActiveClusters(&clusters, alto::limb_gemm_pair_kernel<256, alto::Epi::kScan>, &cfg) !=
-            cudaSuccess ||
-        clusters <= 0)
-      clusters = sms / 2;
-    cudaGetLastError();
-    cached = clusters;
-  }
-  return cached;
+  static const int pairs = compute_resident_pairs();  // thread-safe one-time initialisation
+  return pairs;
 }
 
 int pick_bn(size_t limb_cols) {
@@ -317,6 +348,8 @@ int pick_bn(size_t limb_cols) {
 
 struct Plan {
   bool pair = false;  // CTA-pair kernels (limb columns > 16) or the single-CTA kernels
+  bool wide = false;  // scan units of 512 limb columns (one read of each database tile for all of them)
+  int scan_n = 1;     // scan tiles along the limb columns (num_n / 2 when wide)
   int kb_chunk = 1;   // scan blocks per record chunk
   int bn = 16, num_n = 1;
   int scan_m = 0, scan_split = 1, scan_kb_per = 1, scan_kb = 0;
@@ -365,9 +398,14 @@ Plan make_plan(const Engine *e, size_t slots) {
   p.scan_m = (int)((e->cols + 255) / 256);
   p.pack_m = (int)((4 * e->cols + 255) / 256);
   const int pairs = resident_pairs();
+  // Wide scan units once the database spans several record chunks (its tiles then stream from HBM and cannot be
+  // shared between two pairs through L2) and there are at least 512 limb columns; ALTO_SCAN_WIDE=0/1 overrides.
+  p.wide = p.bn == 256 && p.num_n >= 2 && e->nchunks > 1;
+  if (const char *w = getenv("ALTO_SCAN_WIDE")) p.wide = p.bn == 256 && p.num_n >= 2 && w[0] == '1';
+  p.scan_n = p.wide ? (p.num_n + 1) / 2 : p.num_n;
   // Scan chunks: at most 256 blocks (exactness, as above), at least 8, and about twelve units per resident pair so
   // the persistent pairs finish together.
-  const long tiles = (long)p.scan_m * p.num_n;
+  const long tiles = (long)p.scan_m * p.scan_n;
   long split = std::max<long>((p.scan_kb + 255) / 256, (12L * pairs + tiles - 1) / tiles);
   split = std::min<long>(split, std::max<long>(1, p.scan_kb / 8));
   split = std::max<long>(split, (p.scan_kb + 255) / 256);
@@ -380,25 +418,25 @@ Plan make_plan(const Engine *e, size_t slots) {
 
 // The scan GEMM (acc sums, pre-zeroed) and the pack GEMM (beta) for `slots` clients under plan p.
 bool launch_scan(const Engine *e, const Plan &p, const CUtensorMap &map_q, uint32_t *acc, size_t slots,
-                 cudaStream_t st) {
+                 cudaStream_t st, uint32_t *err) {
   // The query limbs are re-read by every unit of a K chunk; mark them evict-last only while the whole operand
   // (4 bytes per record and client) is a small part of the 126 MB L2, so stale chunks never crowd it out.
   const int keep_b = 4 * round_up(slots, 4) * e->rows <= (size_t(32) << 20);
   if (p.pair) {
     alto::PairArgs g;
     g.num_m = p.scan_m;
-    g.num_n = p.num_n;
-    g.num_units = p.scan_m * p.num_n * p.scan_split;
+    g.num_n = p.scan_n;
+    g.num_units = p.scan_m * p.scan_n * p.scan_split;
     g.kb_total = p.scan_kb;
     g.kb_per_unit = p.scan_kb_per;
     g.rows_a = (int)e->cols;
     g.clients = (int)slots;
     g.cols = (int)e->cols;
     g.out = acc;
-    g.err = e->d_err;
+    g.err = err;
     g.b_keep = keep_b;
     g.kb_chunk = p.kb_chunk;
-    return dispatch_pair<alto::Epi::kScan>(p.bn, e->map_db, map_q, g, p.pairs_scan, st);
+    return dispatch_pair<alto::Epi::kScan>(p.bn, e->map_db, map_q, g, p.pairs_scan, st, p.wide);
   }
   alto::GemmArgs g;
   g.num_m = p.scan_m;
@@ -409,14 +447,14 @@ bool launch_scan(const Engine *e, const Plan &p, const CUtensorMap &map_q, uint3
   g.clients = (int)slots;
   g.cols = (int)e->cols;
   g.out = acc;
-  g.err = e->d_err;
+  g.err = err;
   g.b_keep = keep_b;
   g.kb_chunk = p.kb_chunk;
   return dispatch_gemm<alto::Epi::kScan>(p.bn, e->map_db, map_q, g, p.scan_m * p.num_n * p.scan_split, st);
 }
 
 bool launch_pack(const Engine *e, const Plan &p, const CUtensorMap &map_y, uint32_t *beta, size_t slots,
-                 cudaStream_t st) {
+                 cudaStream_t st, uint32_t *err) {
   const int keep_b = 4 * round_up(slots, 4) * e->count <= (size_t(32) << 20);
   if (p.pair) {
     alto::PairArgs g;
@@ -429,7 +467,7 @@ bool launch_pack(const Engine *e, const Plan &p, const CUtensorMap &map_y, uint3
     g.clients = (int)slots;
     g.cols = (int)e->cols;
     g.out = beta;
-    g.err = e->d_err;
+    g.err = err;
     g.b_keep = keep_b;
     g.kb_chunk = 1;
     return dispatch_pair<alto::Epi::kPack>(p.bn, e->map_ub, map_y, g, p.pairs_pack, st);
@@ -443,7 +481,7 @@ bool launch_pack(const Engine *e, const Plan &p, const CUtensorMap &map_y, uint3
   g.clients = (int)slots;
   g.cols = (int)e->cols;
   g.out = beta;
-  g.err = e->d_err;
+  g.err = err;
   g.b_keep = keep_b;
   g.kb_chunk = 1;
   return dispatch_gemm<alto::Epi::kPack>(p.bn, e->map_ub, map_y, g, p.pack_m * p.num_n, st);
@@ -463,57 +501,62 @@ bool make_limb_maps(const Engine *e, const Plan &p, const uint8_t *qlimb, const 
 // scan GEMM and tail.  The pack needs only the keys, so it overlaps the upload of the much larger query words.
 // Statuses go to d_status (and to the pinned host copy when host_status); responses of valid frames to
 // resp + slot * resp_stride.
-bool enqueue_batch(Engine *e, const uint8_t *d_slots, size_t slot_stride, size_t slots, uint8_t *resp,
+bool enqueue_batch(Engine *e, Batch *bt, const uint8_t *d_slots, size_t slot_stride, size_t slots, uint8_t *resp,
                    size_t resp_stride, bool host_status, cudaEvent_t queries_ready = nullptr) {
-  cudaStream_t st = e->st;
+  cudaStream_t st = bt->st;
   const Plan p = make_plan(e, slots);
   const int bp = (int)round_up(slots, 4);
   int launches = 0;
-  int set = 0;
-  if (!next_set(e, &set)) return false;
-  cudaEvent_t *mk = e->marks[set];
-  // marks: 0 begin | validate | 1 | y split | 2 | pack | 3 | (query wait) q split, zeroing | 4 | scan | 5 | tail | 6
-  ALTO_CK(cudaEventRecord(mk[0], st));
+  // timing marks (main batch only): 0 begin | validate | 1 | y split | 2 | pack | 3 | (query wait) q split,
+  // zeroing | 4 | scan | 5 | tail | 6
+  cudaEvent_t *mk = nullptr;
+  if (bt->timing) {
+    int set = 0;
+    if (!next_set(e, &set)) return false;
+    mk = e->marks[set];
+  }
+  auto mark = [&](int i) { return mk ? cudaEventRecord(mk[i], st) : cudaSuccess; };
+  ALTO_CK(mark(0));
 
   alto::validate_kernel<<<(unsigned)slots, 256, 0, st>>>(d_slots, slot_stride, kSlotLead, e->count, e->rows,
-                                                         e->d_status);
+                                                         bt->d_status);
   ++launches;
   ALTO_CK(cudaGetLastError());
-  if (host_status) ALTO_CK(cudaMemcpyAsync(e->h_status, e->d_status, slots * sizeof(int), cudaMemcpyDeviceToHost, st));
-  ALTO_CK(cudaEventRecord(mk[1], st));
+  if (host_status) ALTO_CK(cudaMemcpyAsync(bt->h_status, bt->d_status, slots * sizeof(int), cudaMemcpyDeviceToHost, st));
+  ALTO_CK(mark(1));
 
   CUtensorMap map_q, map_y;
-  if (!make_limb_maps(e, p, e->d_qlimb, e->d_ylimb, bp, &map_q, &map_y)) return false;
+  if (!make_limb_maps(e, p, bt->d_qlimb, bt->d_ylimb, bp, &map_q, &map_y)) return false;
   const unsigned split_threads = 256;
   {
     const size_t work = (e->count / 16) * (size_t)bp;
     alto::limb_split_kernel<<<(unsigned)((work + split_threads - 1) / split_threads), split_threads, 0, st>>>(
-        d_slots, slot_stride, kSlotLead + 9, (int)slots, bp, e->count, e->count, e->d_ylimb);
+        d_slots, slot_stride, kSlotLead + 9, (int)slots, bp, e->count, e->count, bt->d_ylimb);
     ++launches;
     ALTO_CK(cudaGetLastError());
   }
-  ALTO_CK(cudaEventRecord(mk[2], st));
-  if (!launch_pack(e, p, map_y, e->d_beta, slots, st)) return false;
+  ALTO_CK(mark(2));
+  if (!launch_pack(e, p, map_y, bt->d_beta, slots, st, bt->d_err)) return false;
   ++launches;
-  ALTO_CK(cudaEventRecord(mk[3], st));
+  ALTO_CK(mark(3));
   if (queries_ready) ALTO_CK(cudaStreamWaitEvent(st, queries_ready, 0));
   {
     const size_t work = (e->rows / 16) * (size_t)bp;
     alto::limb_split_kernel<<<(unsigned)((work + split_threads - 1) / split_threads), split_threads, 0, st>>>(
-        d_slots, slot_stride, kSlotLead + 9 + 8 * e->count, (int)slots, bp, e->rows, e->chunk, e->d_qlimb);
+        d_slots, slot_stride, kSlotLead + 9 + 8 * e->count, (int)slots, bp, e->rows, e->chunk, bt->d_qlimb);
     ++launches;
     ALTO_CK(cudaGetLastError());
   }
-  ALTO_CK(cudaMemsetAsync(e->d_acc, 0, slots * e->cols * sizeof(uint32_t), st));
-  ALTO_CK(cudaEventRecord(mk[4], st));
-  if (!launch_scan(e, p, map_q, e->d_acc, slots, st)) return false;
+  ALTO_CK(cudaMemsetAsync(bt->d_acc, 0, slots * e->cols * sizeof(uint32_t), st));
+  ALTO_CK(mark(4));
+  if (!launch_scan(e, p, map_q, bt->d_acc, slots, st, bt->d_err)) return false;
   ++launches;
-  ALTO_CK(cudaEventRecord(mk[5], st));
+  ALTO_CK(mark(5));
   {
     alto::TailArgs t;
-    t.acc = e->d_acc;
-    t.beta = e->d_beta;
-    t.status = e->d_status;
+    t.acc = bt->d_acc;
+    t.beta = bt->d_beta;
+    t.status = bt->d_status;
     t.req = d_slots;
     t.req_stride = slot_stride;
     t.z_off = kSlotLead + 9 + 4 * e->count;
@@ -533,7 +576,7 @@ bool enqueue_batch(Engine *e, const uint8_t *d_slots, size_t slot_stride, size_t
     ALTO_CK(alto::launch_tail(t, slots, st));
     ++launches;
   }
-  ALTO_CK(cudaEventRecord(mk[6], st));
+  ALTO_CK(mark(6));
   e->last_launches = launches;
   return true;
 }
@@ -570,12 +613,12 @@ bool copy_runs(size_t items, size_t width, SrcAt src_at, DstAt dst_at, cudaMemcp
 // Waits for the engine's stream, folds pending timing marks into the totals and checks (then clears) the device
 // error word.
 bool sync_engine(Engine *e) {
-  ALTO_CK(cudaMemcpyAsync(e->h_err, e->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->st));
-  ALTO_CK(cudaStreamSynchronize(e->st));
-  const uint32_t err = *e->h_err;
+  ALTO_CK(cudaMemcpyAsync(e->main.h_err, e->main.d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->main.st));
+  ALTO_CK(cudaStreamSynchronize(e->main.st));
+  const uint32_t err = *e->main.h_err;
   if (err) {
-    ALTO_CK(cudaMemsetAsync(e->d_err, 0, sizeof(uint32_t), e->st));
-    ALTO_CK(cudaStreamSynchronize(e->st));
+    ALTO_CK(cudaMemsetAsync(e->main.d_err, 0, sizeof(uint32_t), e->main.st));
+    ALTO_CK(cudaStreamSynchronize(e->main.st));
     char buf[96];
     snprintf(buf, sizeof buf, "a kernel wait timed out (device error word 0x%x)", err);
     set_error(buf);
@@ -639,25 +682,25 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
     }
     return -3;
   }
-  if (cudaSetDevice(e->dev) != cudaSuccess || !ensure_capacity(e, cand.size())) return -4;
-  cudaStream_t st = e->st;
+  if (cudaSetDevice(e->dev) != cudaSuccess || !ensure_capacity(e, &e->main, cand.size())) return -4;
+  cudaStream_t st = e->main.st;
   if (cudaEventRecord(e->ev_begin, st) != cudaSuccess) return -4;
   // header and keys first on the compute stream, then the query words on the copy stream, so that validation and
   // the pack run while the queries are still uploading
   const size_t head = 9 + 8 * e->count;
   if (!copy_runs(
           cand.size(), head, [&](size_t i) { return (const void *)req[cand[i]]; },
-          [&](size_t i) { return (void *)(e->d_req + i * e->slot_stride + kSlotLead); }, cudaMemcpyHostToDevice, st))
+          [&](size_t i) { return (void *)(e->main.d_req + i * e->slot_stride + kSlotLead); }, cudaMemcpyHostToDevice, st))
     return -4;
   if (cudaEventRecord(e->ev_keys, st) != cudaSuccess || cudaStreamWaitEvent(e->st_copy, e->ev_keys, 0) != cudaSuccess)
     return -4;
   if (!copy_runs(
           cand.size(), e->want - head, [&](size_t i) { return (const void *)(req[cand[i]] + head); },
-          [&](size_t i) { return (void *)(e->d_req + i * e->slot_stride + kSlotLead + head); },
+          [&](size_t i) { return (void *)(e->main.d_req + i * e->slot_stride + kSlotLead + head); },
           cudaMemcpyHostToDevice, e->st_copy))
     return -4;
   if (cudaEventRecord(e->ev_queries, e->st_copy) != cudaSuccess) return -4;
-  if (!enqueue_batch(e, e->d_req, e->slot_stride, cand.size(), e->d_resp, e->resp_len, true, e->ev_queries))
+  if (!enqueue_batch(e, &e->main, e->main.d_req, e->slot_stride, cand.size(), e->main.d_resp, e->resp_len, true, e->ev_queries))
     return -4;
   if (cudaEventSynchronize(e->marks[e->last_set][1]) != cudaSuccess) {
     set_error("status event failed");
@@ -665,11 +708,11 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
   }
   std::vector<size_t> ok;  // indices into cand with status 0
   for (size_t i = 0; i < cand.size(); ++i) {
-    status[cand[i]] = e->h_status[i];
-    if (e->h_status[i] == 0) ok.push_back(i);
+    status[cand[i]] = e->main.h_status[i];
+    if (e->main.h_status[i] == 0) ok.push_back(i);
   }
   if (!copy_runs(
-          ok.size(), e->resp_len, [&](size_t k) { return (const void *)(e->d_resp + ok[k] * e->resp_len); },
+          ok.size(), e->resp_len, [&](size_t k) { return (const void *)(e->main.d_resp + ok[k] * e->resp_len); },
           [&](size_t k) { return (void *)out[cand[ok[k]]]; }, cudaMemcpyDeviceToHost, st))
     return -4;
   if (cudaEventRecord(e->ev_end, st) != cudaSuccess) return -4;
@@ -736,7 +779,10 @@ void *alto_engine_new(const uint8_t *db_col, const uint8_t *db_tiled, size_t ld,
   };
   cudaError_t err;
   if ((err = cudaGetDevice(&e->dev)) != cudaSuccess) return fail("cudaGetDevice", err);
-  if ((err = cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking)) != cudaSuccess) return fail("stream", err);
+  if (!init_batch(&e->main, true)) {
+    destroy(e);
+    return nullptr;
+  }
   if ((err = cudaStreamCreateWithFlags(&e->st_copy, cudaStreamNonBlocking)) != cudaSuccess) return fail("stream", err);
   if ((err = cudaEventCreate(&e->ev_begin)) != cudaSuccess || (err = cudaEventCreate(&e->ev_end)) != cudaSuccess ||
       (err = cudaEventCreateWithFlags(&e->ev_keys, cudaEventDisableTiming)) != cudaSuccess ||
@@ -779,10 +825,6 @@ void *alto_engine_new(const uint8_t *db_col, const uint8_t *db_tiled, size_t ld,
     if (!pre.empty() && (err = cudaMemcpy(e->d_prefix, pre.data(), pre.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
       return fail("prefix upload", err);
   }
-  if ((err = cudaMalloc(&e->d_err, sizeof(uint32_t))) != cudaSuccess) return fail("error word", err);
-  if ((err = cudaMemset(e->d_err, 0, sizeof(uint32_t))) != cudaSuccess) return fail("error word", err);
-  if ((err = cudaHostAlloc(&e->h_err, sizeof(uint32_t), cudaHostAllocDefault)) != cudaSuccess)
-    return fail("pinned error word", err);
   if (!make_map3(&e->map_db, e->d_db, e->chunk, cols, e->nchunks, alto::kBM) ||
       !make_map(&e->map_ub, e->d_ub, e->count, 4 * cols, e->count, alto::kBM)) {
     destroy(e);
@@ -820,14 +862,14 @@ int alto_answer_device(void *p, const uint8_t *d_req, size_t req_stride, size_t 
   e->last_launches = 0;
   if (!b) return 0;
   if (!e->tail_ok) return -3;
-  if (cudaSetDevice(e->dev) != cudaSuccess || !ensure_capacity(e, b)) return -4;
-  if (cudaEventRecord(e->ev_begin, e->st) != cudaSuccess) return -4;
-  if (!enqueue_batch(e, d_req, req_stride, b, d_out, out_stride, true)) return -4;
-  if (cudaEventRecord(e->ev_end, e->st) != cudaSuccess) return -4;
+  if (cudaSetDevice(e->dev) != cudaSuccess || !ensure_capacity(e, &e->main, b)) return -4;
+  if (cudaEventRecord(e->ev_begin, e->main.st) != cudaSuccess) return -4;
+  if (!enqueue_batch(e, &e->main, d_req, req_stride, b, d_out, out_stride, true)) return -4;
+  if (cudaEventRecord(e->ev_end, e->main.st) != cudaSuccess) return -4;
   if (!finish(e, stage_ms)) return -4;
   int valid = 0;
   for (size_t c = 0; c < b; ++c) {
-    status[c] = e->h_status[c];
+    status[c] = e->main.h_status[c];
     valid += status[c] == 0;
   }
   return valid;
@@ -842,10 +884,10 @@ int alto_enqueue_device(void *p, const uint8_t *d_req, size_t req_stride, size_t
   e->last_launches = 0;
   if (!b) return 0;
   if (!e->tail_ok) return -3;
-  if (cudaSetDevice(e->dev) != cudaSuccess || !ensure_capacity(e, b)) return -4;
-  if (!enqueue_batch(e, d_req, req_stride, b, d_out, out_stride, false)) return -4;
+  if (cudaSetDevice(e->dev) != cudaSuccess || !ensure_capacity(e, &e->main, b)) return -4;
+  if (!enqueue_batch(e, &e->main, d_req, req_stride, b, d_out, out_stride, false)) return -4;
   if (d_status &&
-      cudaMemcpyAsync(d_status, e->d_status, b * sizeof(int), cudaMemcpyDeviceToDevice, e->st) != cudaSuccess) {
+      cudaMemcpyAsync(d_status, e->main.d_status, b * sizeof(int), cudaMemcpyDeviceToDevice, e->main.st) != cudaSuccess) {
     set_error("status copy failed");
     return -4;
   }
@@ -859,7 +901,7 @@ int alto_engine_sync(void *p) {
   return sync_engine(e) ? 0 : -4;
 }
 
-void *alto_engine_stream(void *p) { return p ? static_cast<void *>(static_cast<Engine *>(p)->st) : nullptr; }
+void *alto_engine_stream(void *p) { return p ? static_cast<void *>(static_cast<Engine *>(p)->main.st) : nullptr; }
 
 int alto_kernel_times(void *p, double *ms, long long *batches, int reset) {
   Engine *e = static_cast<Engine *>(p);
@@ -958,7 +1000,7 @@ NoAllocLayout noalloc_layout(const Engine *e, size_t b) {
 // static array; statuses are copied to the caller's device array.
 bool enqueue_noalloc(Engine *e, uint8_t *scratch, const NoAllocLayout &l, const uint8_t *d_slots, size_t stride,
                      size_t b, uint8_t *resp, size_t resp_stride, int *d_status) {
-  cudaStream_t st = e->st;
+  cudaStream_t st = e->main.st;
   const Plan p = make_plan(e, b);
   const int bp = (int)round_up(b, 4);
   int *status = reinterpret_cast<int *>(scratch + l.status);
@@ -979,8 +1021,8 @@ bool enqueue_noalloc(Engine *e, uint8_t *scratch, const NoAllocLayout &l, const 
   ALTO_CK(cudaGetLastError());
   CUtensorMap map_q, map_y;
   if (!make_limb_maps(e, p, qlimb, ylimb, bp, &map_q, &map_y)) return false;
-  if (!launch_scan(e, p, map_q, acc, b, st)) return false;
-  if (!launch_pack(e, p, map_y, beta, b, st)) return false;
+  if (!launch_scan(e, p, map_q, acc, b, st, e->main.d_err)) return false;
+  if (!launch_pack(e, p, map_y, beta, b, st, e->main.d_err)) return false;
   alto::TailArgs t;
   t.acc = acc;
   t.beta = beta;
@@ -1032,18 +1074,20 @@ extern "C" int alto_answer_device_noalloc(void *p, const uint8_t *d_req, size_t 
   if (!noalloc_scratch(e->dev, &scratch)) return -4;
   if (!enqueue_noalloc(e, scratch, l, d_req, req_stride, b, d_out, out_stride, d_status)) return -4;
   // wait and check the engine's device error word (its pinned host mirror already exists)
-  if (cudaMemcpyAsync(e->h_err, e->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->st) != cudaSuccess ||
-      cudaStreamSynchronize(e->st) != cudaSuccess) {
+  if (cudaMemcpyAsync(e->main.h_err, e->main.d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->main.st) != cudaSuccess ||
+      cudaStreamSynchronize(e->main.st) != cudaSuccess) {
     set_error("allocation-free batch failed", cudaGetLastError());
     return -4;
   }
-  if (*e->h_err) {
+  if (*e->main.h_err) {
     char buf[96];
-    snprintf(buf, sizeof buf, "a kernel wait timed out (device error word 0x%x)", *e->h_err);
+    snprintf(buf, sizeof buf, "a kernel wait timed out (device error word 0x%x)", *e->main.h_err);
     set_error(buf);
-    cudaMemsetAsync(e->d_err, 0, sizeof(uint32_t), e->st);
-    cudaStreamSynchronize(e->st);
+    cudaMemsetAsync(e->main.d_err, 0, sizeof(uint32_t), e->main.st);
+    cudaStreamSynchronize(e->main.st);
     return -4;
   }
   return 0;
 }
+
+#include "serving.cuh"

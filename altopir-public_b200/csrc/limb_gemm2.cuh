@@ -20,18 +20,24 @@
 
 namespace alto {
 
-template <int BN>
+// NSUB = 1: a unit is BN limb columns and TMEM holds two accumulators (the epilogue of one unit overlaps the
+// MMAs of the next).  NSUB = 2: a unit is 2 x BN limb columns in two sub-accumulators that fill TMEM (one buffer),
+// so that every A tile is read once for all of them -- for long scans whose A tiles are too large to be shared
+// between pairs through L2.
+template <int BN, int NSUB = 1>
 struct PairShape {
   static constexpr int kABytes = 128 * kBK;                 // this CTA's 128 rows of A
-  static constexpr int kBBytes = (BN / 2) * kBK;            // this CTA's BN/2 rows of B
+  static constexpr int kBBytes = NSUB * (BN / 2) * kBK;     // this CTA's BN/2 rows of B for each sub-tile
   static constexpr int kStageBytes = kABytes + kBBytes;
   static constexpr int kStages = (196608 / kStageBytes) < 8 ? (196608 / kStageBytes) : 8;
-  static constexpr int kTmemCols = 2 * BN;                  // two accumulators of BN columns
+  static constexpr int kBufs = NSUB == 1 ? 2 : 1;           // accumulator buffers
+  static constexpr int kTmemCols = kBufs * NSUB * BN;
   static constexpr int kBarrierBytes = 512;
   static constexpr int kSmemBytes = kStages * kStageBytes + kBarrierBytes + 1024;
   static_assert(BN % 32 == 0 && BN >= 32 && BN <= 256, "pair kind::i8 MMA needs N in [32, 256], N % 32 == 0");
   static_assert(kStageBytes % 1024 == 0, "stages must keep 1024-byte swizzle-atom alignment");
   static_assert(kStages >= 3, "pipeline depth");
+  static_assert(kTmemCols <= 512, "TMEM has 512 columns");
 };
 
 struct PairArgs {
@@ -80,18 +86,19 @@ __device__ __forceinline__ void pack_epilogue16(const uint32_t (&r)[16], int gro
   }
 }
 
-template <int BN, Epi EPI>
+template <int BN, Epi EPI, int NSUB = 1>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
     limb_gemm_pair_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
                           PairArgs args) {
-  using S = PairShape<BN>;
+  using S = PairShape<BN, NSUB>;
+  constexpr int kBufs = S::kBufs;
   constexpr int kStages = S::kStages;
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw_addr = smem_u32(smem_raw);
   const uint32_t base_addr = (raw_addr + 1023u) & ~1023u;
   uint8_t *smem = smem_raw + (base_addr - raw_addr);
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kStages * S::kStageBytes);
-  // bars: [0, S) full, [S, 2S) empty, 2S + b acc_full[b], 2S + 2 + b acc_empty[b]
+  // bars: [0, S) full, [S, 2S) empty, 2S + b acc_full[b], 2S + 2 + b acc_empty[b] (b < kBufs)
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * kStages + 4);
   volatile int *bail = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
@@ -159,11 +166,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
           if constexpr (EPI == Epi::kScan) {
             const int kb = kb0 + i, z = kb / args.kb_chunk, x = (kb - z * args.kb_chunk) * kBK;
             tma_load_3d_pair(sa, &map_a, full_leader0 + 8 * s, x, m * 256 + (int)rank * 128, z, pol_a);
-            tma_load_3d_pair(sb, &map_b, full_leader0 + 8 * s, x, n * BN + (int)rank * (BN / 2), z, pol_b);
+#pragma unroll
+            for (int t = 0; t < NSUB; ++t)
+              tma_load_3d_pair(sb + t * (BN / 2) * kBK, &map_b, full_leader0 + 8 * s, x,
+                               (n * NSUB + t) * BN + (int)rank * (BN / 2), z, pol_b);
           } else {
             const int x = (kb0 + i) * kBK;
             tma_load_2d_pair(sa, &map_a, full_leader0 + 8 * s, x, m * 256 + (int)rank * 128, pol_a);
-            tma_load_2d_pair(sb, &map_b, full_leader0 + 8 * s, x, n * BN + (int)rank * (BN / 2), pol_b);
+#pragma unroll
+            for (int t = 0; t < NSUB; ++t)
+              tma_load_2d_pair(sb + t * (BN / 2) * kBK, &map_b, full_leader0 + 8 * s, x,
+                               (n * NSUB + t) * BN + (int)rank * (BN / 2), pol_b);
           }
         }
       }
@@ -184,10 +197,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
       for (int u = pair; u < args.num_units && !stop; u += pairs, ++it) {
         int m, n, kb0, nkb;
         unit_coords(u, m, n, kb0, nkb);
-        const int ab = it & 1, use = it >> 1;
+        const int ab = it % kBufs, use = it / kBufs;
         if (use > 0 && !mbar_wait(acce0 + 8 * ab, (use - 1) & 1, args.err, ALTO_ERR_WAIT_ACCUM, bail)) break;
         tc_fence_after();
-        const uint32_t d_tmem = tmem_base + (uint32_t)(ab * BN);
+        const uint32_t d_tmem = tmem_base + (uint32_t)(ab * NSUB * BN);
         for (int i = 0; i < nkb; ++i, ++g) {
           const int s = g % kStages, round = g / kStages;
           if (!mbar_wait(full0 + 8 * s, round & 1, args.err, ALTO_ERR_WAIT_FULL, bail)) {
@@ -197,8 +210,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
           tc_fence_after();
           const uint32_t sa = base_addr + s * S::kStageBytes, sb = sa + S::kABytes;
 #pragma unroll
-          for (int kk = 0; kk < kBK / 32; ++kk)
-            mma_i8_pair(d_tmem, desc_sw128(sa + kk * 32), desc_sw128(sb + kk * 32), idesc, (i | kk) != 0);
+          for (int t = 0; t < NSUB; ++t)
+#pragma unroll
+            for (int kk = 0; kk < kBK / 32; ++kk)
+              mma_i8_pair(d_tmem + t * BN, desc_sw128(sa + kk * 32), desc_sw128(sb + t * (BN / 2) * kBK + kk * 32),
+                          idesc, (i | kk) != 0);
           mma_commit_pair(empty0 + 8 * s);
         }
         mma_commit_pair(accf0 + 8 * ab);
@@ -221,18 +237,18 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
     for (int u = pair; u < args.num_units; u += pairs, ++it) {
       int m, n, kb0, nkb;
       unit_coords(u, m, n, kb0, nkb);
-      const int ab = it & 1, use = it >> 1;
+      const int ab = it % kBufs, use = it / kBufs;
       if (!mbar_wait(accf0 + 8 * ab, use & 1, args.err, ALTO_ERR_WAIT_ACCUM, bail)) break;
       tc_fence_after();
-      const uint32_t taddr = tmem_base + (uint32_t)(ab * BN) + ((uint32_t)(q * 32) << 16);
+      const uint32_t taddr = tmem_base + (uint32_t)(ab * NSUB * BN) + ((uint32_t)(q * 32) << 16);
       const int grow = m * 256 + (int)rank * 128 + row;
       const bool row_ok = grow < args.rows_a;
 #pragma unroll 1
-      for (int ch = 0; ch < BN / 16; ++ch) {
+      for (int ch = 0; ch < NSUB * BN / 16; ++ch) {
         uint32_t r[16];
         tmem_ld16(taddr + ch * 16, r);
         tmem_wait_ld();
-        const int c0 = n * (BN / 4) + ch * 4;
+        const int c0 = n * NSUB * (BN / 4) + ch * 4;
         if constexpr (EPI == Epi::kScan)
           scan_epilogue16(r, grow, row_ok, c0, args.clients, args.cols, args.out);
         else

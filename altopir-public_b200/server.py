@@ -1,0 +1,93 @@
+"""Serving loop with continuous batching (alto_server_*): the engine loop of the reference's server
+(src/bin/altopir.rs:245-513) without its TCP front end, plus an open-loop Poisson load generator."""
+import ctypes
+import threading
+import time
+
+import numpy as np
+
+from . import lib, last_error
+
+BUSY = -9       # alto_server_submit: the queue is full (the reference server's status 9)
+TIMEOUT = -5    # alto_server_wait: not done within the timeout
+FAILED = -4     # device failure
+
+
+class Server:
+    """A serving loop on an engine (engine.Engine), or on the host loopback executor when engine is None."""
+
+    def __init__(self, engine=None, max_batch=128, queue_cap=512, slots=3, request_len=None, response_len=None,
+                 service_us=0.0):
+        if engine is not None:
+            self.ptr = lib().alto_server_new(engine.ptr, max_batch, queue_cap, slots)
+            self.response_len = engine.response_len()
+            self.request_len = engine.request_len()
+        else:
+            self.ptr = lib().alto_server_new_loopback(request_len, response_len, max_batch, queue_cap, slots,
+                                                      float(service_us))
+            self.response_len, self.request_len = response_len, request_len
+        if not self.ptr:
+            raise RuntimeError(f"serving loop not created: {last_error()}")
+        self._engine = engine  # the engine must outlive the loop
+
+    def submit(self, frame):
+        """Queue one frame (uint8 array); returns a ticket >= 0 or BUSY."""
+        f = np.ascontiguousarray(frame, dtype=np.uint8)
+        return lib().alto_server_submit(self.ptr, ctypes.c_void_p(f.ctypes.data), f.size)
+
+    def wait(self, ticket, timeout_ms=60000):
+        """(status, response or None) of a ticket; status as alto_server_wait."""
+        out = np.empty(self.response_len, dtype=np.uint8)
+        st = lib().alto_server_wait(self.ptr, ticket, ctypes.c_void_p(out.ctypes.data), out.size, timeout_ms)
+        return st, (out if st == 0 else None)
+
+    def stats(self):
+        v = (ctypes.c_double * 11)()
+        lib().alto_server_stats(self.ptr, v, 11)
+        keys = ("answered", "rejected", "busy", "failed", "batches", "mean_batch", "p50_ms", "p99_ms", "p999_ms",
+                "max_ms", "queued")
+        return dict(zip(keys, list(v)))
+
+    def close(self):
+        if getattr(self, "ptr", None):
+            lib().alto_server_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        self.close()
+
+
+def poisson_load(server, frames, rate_qps, seconds, seed=1, clients=4):
+    """Open-loop load: arrival times drawn from a Poisson process of rate_qps over `seconds`, frames taken round
+    robin from `frames`, submitted by `clients` threads at their due times; each thread then waits for its tickets.
+    Returns (results, offered) with results[i] = (frame index, status, response, latency_s)."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate_qps, size=int(rate_qps * seconds * 1.5) + 8))
+    t = t[t < seconds]
+    results = [None] * len(t)
+    start = time.perf_counter() + 0.05
+
+    def worker(k):
+        mine = []
+        for i in range(k, len(t), clients):
+            due = start + t[i]
+            while True:
+                d = due - time.perf_counter()
+                if d <= 0:
+                    break
+                time.sleep(min(d, 0.002))
+            t0 = time.perf_counter()
+            mine.append((i, server.submit(frames[i % len(frames)]), t0))
+        for i, ticket, t0 in mine:
+            if ticket < 0:
+                results[i] = (i % len(frames), ticket, None, 0.0)
+                continue
+            st, resp = server.wait(ticket)
+            results[i] = (i % len(frames), st, resp, time.perf_counter() - t0)
+
+    th = [threading.Thread(target=worker, args=(k,)) for k in range(clients)]
+    for x in th:
+        x.start()
+    for x in th:
+        x.join()
+    return results, len(t)

@@ -40,6 +40,11 @@ def parse():
     ap.add_argument("--batch", type=int, default=128)
     ap.add_argument("--plain-queries", type=int, default=128, help="single-query launches timed for the plain path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve", type=str, default=None,
+                    help="serving mode: comma-separated offered rates in QPS (open-loop Poisson arrivals)")
+    ap.add_argument("--serve-seconds", type=float, default=3.0)
+    ap.add_argument("--serve-clients", type=int, default=4096, help="seeded clients whose frames are replayed")
+    ap.add_argument("--max-batch", type=int, default=1024)
     return ap.parse_args()
 
 
@@ -215,6 +220,49 @@ def main_reference(a):
             "config": config_dict(a), "cpu_baseline": dict(info, value=qps, unit="QPS"),
             "e2e": {"value": qps, "unit": "QPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------------------------------------ serving mode
+def main_serve(a):
+    """Open-loop serving: Poisson arrivals at each offered rate into the continuous-batching loop (max_batch
+    a.max_batch, three device batch contexts) and into a one-query-per-batch loop, answered QPS and latency
+    percentiles from submit to completion.  One JSON line."""
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    import __graft_entry__ as ge
+    ge.load()
+    from altopir_b200 import engine as eng, service as svc, server as srv
+    eng.init()
+    p = svc.params(a.rows, a.record_bytes)
+    st = svc.SyntheticState.make(p, seed=1, keep_values=False)
+    e = eng.Engine.from_state(st, threads=svc.threads(), tile=a.rows * a.record_bytes <= (8 << 30))
+    st.ub = None
+    frames = svc.synthetic_requests(p, a.serve_clients, seed=2024)
+    rates = [float(x) for x in a.serve.split(",")]
+    rows = []
+    for label, mb in (("batched", a.max_batch), ("plain", 1)):
+        s = srv.Server(e, max_batch=mb, queue_cap=max(4 * a.max_batch, 4096), slots=3)
+        for rate in rates:
+            s.stats()
+            res, offered = srv.poisson_load(s, frames, rate, a.serve_seconds, seed=int(rate), clients=8)
+            lat = sorted(r[3] * 1e3 for r in res if r[1] == 0)
+            ok = len(lat)
+            pct = lambda q: lat[min(len(lat) - 1, int(q * len(lat)))] if lat else None
+            rows.append({"loop": label, "offered_qps": rate, "requests": offered, "answered": ok,
+                         "busy": sum(1 for r in res if r[1] == srv.BUSY),
+                         "answered_qps": ok / a.serve_seconds, "p50_ms": pct(0.5), "p99_ms": pct(0.99),
+                         "p999_ms": pct(0.999)})
+        rows[-1]["loop_stats"] = s.stats()
+        s.close()
+    line = {"metric": "serving: answered QPS and p50/p99/p99.9 latency (submit to response) under open-loop "
+                      "Poisson arrivals", "unit": "QPS", "n_gpus": 1, "data": "synthetic",
+            "config": {"workload": f"continuous batching over a {a.rows * a.record_bytes / 2**30:g} GiB database, "
+                                   f"{a.serve_clients} seeded clients, {a.serve_seconds} s per rate",
+                       "rows": a.rows, "record_bytes": a.record_bytes, "max_batch": a.max_batch, "slots": 3},
+            "rates": rows}
+    print(json.dumps(line))
+    e.close()
     return 0
 
 
@@ -400,4 +448,6 @@ def main_ours(a):
 
 if __name__ == "__main__":
     args = parse()
+    if args.serve:
+        sys.exit(main_serve(args))
     sys.exit(main_reference(args) if args.impl == "reference" else main_ours(args))

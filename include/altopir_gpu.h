@@ -131,6 +131,32 @@ int alto_kernel_times(void *engine, double *ms, long long *batches, int reset);
 int alto_answer_device_noalloc(void *engine, const uint8_t *d_req, size_t req_stride, size_t b, uint8_t *d_out,
                                size_t out_stride, int *d_status);
 
+/* Serving loop with continuous batching over one engine (the engine loop of src/bin/altopir.rs:245-513 without the
+ * TCP front end).  Frames submitted from any thread wait in a FIFO of queue_cap entries; a batcher thread takes
+ * whatever is queued, up to max_batch, as soon as one of `slots` device batch contexts (1..8) is free -- it never
+ * holds a request back to fill a batch -- and answers it on that context's stream, so up to `slots` batches upload
+ * and compute concurrently.  Each context keeps its frames, limbs, sums and responses resident in device memory,
+ * sized for max_batch frames at creation: admission to the device is by free context.
+ *   alto_server_new        returns NULL for bad arguments (1 <= slots <= 8) or when the device memory is short.
+ *   alto_server_submit     copies the frame and returns a ticket >= 0, -9 when the queue is full (the reference
+ *                          server's BUSY status 9), -1 for bad arguments.
+ *   alto_server_wait       waits up to timeout_ms for a ticket; returns its status (0..3 as alto_answer, with the
+ *                          response copied to out for 0), -4 on a device failure, -5 on timeout (the ticket stays
+ *                          valid), -1 for an unknown ticket.  A completed ticket is released by this call.
+ *   alto_server_stats      out[0..10] = answered, rejected (status 1..3), busy, failed, batches, mean batch size,
+ *                          latency p50, p99, p99.9 and max in ms (submit to completion), frames still queued.
+ *   alto_server_free       answers everything queued, then stops the threads and frees the contexts.
+ * alto_server_new_loopback builds the same loop without an engine: batches are answered on the host after
+ * service_us microseconds by a deterministic function of the frame, to test queueing and batching without a
+ * device.  Both have no counterpart in the reference's C ABI. */
+void *alto_server_new(void *engine, size_t max_batch, size_t queue_cap, int slots);
+void *alto_server_new_loopback(size_t request_len, size_t response_len, size_t max_batch, size_t queue_cap, int slots,
+                               double service_us);
+long long alto_server_submit(void *server, const uint8_t *frame, size_t len);
+int alto_server_wait(void *server, long long ticket, uint8_t *out, size_t out_len, int timeout_ms);
+int alto_server_stats(void *server, double *out, size_t n);
+void alto_server_free(void *server);
+
 /* Deterministic synthetic inputs (test and benchmark data; not part of the answer path).
  * alto_synthetic_db_col: db[(col - col0) * ld + r] = byte col of the reference's synthetic record r
  *   (src/service.rs:43-62, splitmix64 seed 0x416c746f504952), for r < rows and ncols columns from col0.

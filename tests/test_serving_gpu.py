@@ -1,0 +1,37 @@
+"""Continuous batching on the device: requests arriving while others are on the GPU join the next batch, batches
+overlap on the device, and each response is the same as the engine's answer to the request alone."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_each_result_is_the_same_alone_and_in_the_mix(gpu, svc, eng):
+    from altopir_b200 import server as srv
+    import frames as fr
+    p = svc.params(2048, 4096)
+    st = svc.SyntheticState.make(p, seed=71, full_prefix=True)
+    e = eng.Engine.from_state(st)
+    frames = svc.synthetic_requests(p, 48, seed=72)
+    # a few malformed frames mixed in (statuses 1, 2, 3)
+    mf, want = fr.malformed_table(frames[0], frames[1], p.count)
+    mixed = [frames[i] for i in range(48)] + mf[1:7]
+    alone = []
+    for i in range(48):
+        out = np.zeros((1, e.response_len()), dtype=np.uint8)
+        status = np.full(1, -1, dtype=np.int32)
+        assert e.answer([frames[i]], out, status)[0] == 1
+        alone.append(out[0].copy())
+    s = srv.Server(e, max_batch=16, queue_cap=256, slots=3)
+    results, offered = srv.poisson_load(s, mixed, rate_qps=4000, seconds=0.25, seed=73, clients=3)
+    assert offered > 40
+    for idx, status, resp, lat in results:
+        if idx < 48:
+            assert status == 0 and np.array_equal(resp, alone[idx]), idx
+        else:
+            assert status == want[idx - 48 + 1] and resp is None
+    stats = s.stats()
+    assert stats["failed"] == 0 and stats["busy"] == 0 and stats["answered"] > 0 and stats["batches"] > 1
+    assert stats["p50_ms"] > 0 and stats["p99_ms"] >= stats["p50_ms"]
+    s.close()
+    e.close()
