@@ -51,7 +51,7 @@ def _declare(L):
         "alto_server_new": (P, [P, S, S, I]),
         "alto_server_new_loopback": (P, [S, S, S, S, I, c.c_double]),
         "alto_server_submit": (c.c_longlong, [P, P, S]),
-        "alto_server_wait": (I, [P, c.c_longlong, P, S, I]),
+        "alto_server_wait": (I, [P, c.c_longlong, P, S, I, c.POINTER(c.c_double)]),
         "alto_server_stats": (I, [P, c.POINTER(c.c_double), S]),
         "alto_server_free": (None, [P]),
         "alto_synthetic_db_col": (None, [P, S, S, S, S, I]),

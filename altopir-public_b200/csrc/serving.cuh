@@ -311,7 +311,7 @@ long long alto_server_submit(void *p, const uint8_t *frame, size_t len) {
   return id;
 }
 
-int alto_server_wait(void *p, long long id, uint8_t *out, size_t out_len, int timeout_ms) {
+int alto_server_wait(void *p, long long id, uint8_t *out, size_t out_len, int timeout_ms, double *latency_ms) {
   Server *s = static_cast<Server *>(p);
   if (!s) return -1;
   std::unique_lock<std::mutex> lk(s->mu);
@@ -320,6 +320,7 @@ int alto_server_wait(void *p, long long id, uint8_t *out, size_t out_len, int ti
   if (!s->cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return it->second.done; })) return -5;
   const int st = it->second.status;
   if (st == 0 && out) memcpy(out, it->second.resp.data(), std::min(out_len, s->resp_len));
+  if (latency_ms) *latency_ms = 1e3 * (it->second.t_done - it->second.t_submit);
   s->tickets.erase(it);
   return st;
 }

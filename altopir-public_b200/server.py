@@ -35,10 +35,15 @@ class Server:
         f = np.ascontiguousarray(frame, dtype=np.uint8)
         return lib().alto_server_submit(self.ptr, ctypes.c_void_p(f.ctypes.data), f.size)
 
-    def wait(self, ticket, timeout_ms=60000):
-        """(status, response or None) of a ticket; status as alto_server_wait."""
+    def wait(self, ticket, timeout_ms=60000, with_latency=False):
+        """(status, response or None) of a ticket; status as alto_server_wait.  with_latency adds the loop's own
+        submit-to-completion time in ms as a third element."""
         out = np.empty(self.response_len, dtype=np.uint8)
-        st = lib().alto_server_wait(self.ptr, ticket, ctypes.c_void_p(out.ctypes.data), out.size, timeout_ms)
+        lat = ctypes.c_double(0.0)
+        st = lib().alto_server_wait(self.ptr, ticket, ctypes.c_void_p(out.ctypes.data), out.size, timeout_ms,
+                                    ctypes.byref(lat))
+        if with_latency:
+            return st, (out if st == 0 else None), lat.value
         return st, (out if st == 0 else None)
 
     def stats(self):
@@ -59,13 +64,17 @@ class Server:
 
 def poisson_load(server, frames, rate_qps, seconds, seed=1, clients=4):
     """Open-loop load: arrival times drawn from a Poisson process of rate_qps over `seconds`, frames taken round
-    robin from `frames`, submitted by `clients` threads at their due times; each thread then waits for its tickets.
-    Returns (results, offered) with results[i] = (frame index, status, response, latency_s)."""
+    robin from `frames`, submitted by `clients` threads at their due times; each thread then collects its tickets.
+    Returns (results, offered, elapsed_s) with results[i] = (frame index, status, response, latency_s), where the
+    latency is the loop's own time from submit to completion and elapsed_s runs from the first arrival to the last
+    completion."""
     rng = np.random.default_rng(seed)
     t = np.cumsum(rng.exponential(1.0 / rate_qps, size=int(rate_qps * seconds * 1.5) + 8))
     t = t[t < seconds]
     results = [None] * len(t)
     start = time.perf_counter() + 0.05
+    t_first = start
+    done_at = [0.0] * clients
 
     def worker(k):
         mine = []
@@ -76,18 +85,19 @@ def poisson_load(server, frames, rate_qps, seconds, seed=1, clients=4):
                 if d <= 0:
                     break
                 time.sleep(min(d, 0.002))
-            t0 = time.perf_counter()
-            mine.append((i, server.submit(frames[i % len(frames)]), t0))
-        for i, ticket, t0 in mine:
+            mine.append((i, server.submit(frames[i % len(frames)])))
+        for i, ticket in mine:
             if ticket < 0:
                 results[i] = (i % len(frames), ticket, None, 0.0)
                 continue
-            st, resp = server.wait(ticket)
-            results[i] = (i % len(frames), st, resp, time.perf_counter() - t0)
+            st, resp, lat_ms = server.wait(ticket, with_latency=True)
+            results[i] = (i % len(frames), st, resp, lat_ms * 1e-3)
+            done_at[k] = max(done_at[k], t_first + t[i] + lat_ms * 1e-3)
 
     th = [threading.Thread(target=worker, args=(k,)) for k in range(clients)]
     for x in th:
         x.start()
     for x in th:
         x.join()
-    return results, len(t)
+    elapsed = max(max(done_at) - start, seconds) if len(t) else seconds
+    return results, len(t), elapsed

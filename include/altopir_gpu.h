@@ -142,7 +142,8 @@ int alto_answer_device_noalloc(void *engine, const uint8_t *d_req, size_t req_st
  *                          server's BUSY status 9), -1 for bad arguments.
  *   alto_server_wait       waits up to timeout_ms for a ticket; returns its status (0..3 as alto_answer, with the
  *                          response copied to out for 0), -4 on a device failure, -5 on timeout (the ticket stays
- *                          valid), -1 for an unknown ticket.  A completed ticket is released by this call.
+ *                          valid), -1 for an unknown ticket; *latency_ms (if not NULL) receives the time from
+ *                          submit to completion measured by the loop.  A completed ticket is released by this call.
  *   alto_server_stats      out[0..10] = answered, rejected (status 1..3), busy, failed, batches, mean batch size,
  *                          latency p50, p99, p99.9 and max in ms (submit to completion), frames still queued.
  *   alto_server_free       answers everything queued, then stops the threads and frees the contexts.
@@ -153,7 +154,8 @@ void *alto_server_new(void *engine, size_t max_batch, size_t queue_cap, int slot
 void *alto_server_new_loopback(size_t request_len, size_t response_len, size_t max_batch, size_t queue_cap, int slots,
                                double service_us);
 long long alto_server_submit(void *server, const uint8_t *frame, size_t len);
-int alto_server_wait(void *server, long long ticket, uint8_t *out, size_t out_len, int timeout_ms);
+int alto_server_wait(void *server, long long ticket, uint8_t *out, size_t out_len, int timeout_ms,
+                     double *latency_ms);
 int alto_server_stats(void *server, double *out, size_t n);
 void alto_server_free(void *server);
 

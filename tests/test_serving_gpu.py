@@ -23,7 +23,7 @@ def test_each_result_is_the_same_alone_and_in_the_mix(gpu, svc, eng):
         assert e.answer([frames[i]], out, status)[0] == 1
         alone.append(out[0].copy())
     s = srv.Server(e, max_batch=16, queue_cap=256, slots=3)
-    results, offered = srv.poisson_load(s, mixed, rate_qps=4000, seconds=0.25, seed=73, clients=3)
+    results, offered, elapsed = srv.poisson_load(s, mixed, rate_qps=4000, seconds=0.25, seed=73, clients=3)
     assert offered > 40
     for idx, status, resp, lat in results:
         if idx < 48:
