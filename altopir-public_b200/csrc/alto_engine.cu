@@ -7,6 +7,7 @@
 // valid responses only, so rejected output buffers are never touched.
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <dlfcn.h>
 #include <algorithm>
 #include <mutex>
 #include <cstdio>
@@ -126,6 +127,29 @@ struct Batch {
   int *h_status = nullptr;
   uint32_t *d_err = nullptr, *h_err = nullptr;
   bool timing = false;  // record per-kernel timing marks into the engine's ring (main batch only)
+  // CUDA graphs of the device-side launch sequence, one per batch size and buffer set (see enqueue_batch)
+  struct GraphEntry {
+    size_t slots, stride, resp_stride;
+    const uint8_t *d_slots;
+    uint8_t *resp;
+    bool host_status;
+    cudaGraphExec_t exec;
+  };
+  std::vector<GraphEntry> graphs;
+};
+
+void clear_graphs(Batch *b) {
+  for (auto &g : b->graphs) cudaGraphExecDestroy(g.exec);
+  b->graphs.clear();
+}
+
+// One row of a tuning table: the plan knobs for batches of at most b_max frames (0 or -1 = the built-in choice).
+struct TuneEntry {
+  int b_max;
+  int pair;            // 1 CTA-pair kernels, 0 single-CTA kernels, -1 pairs when a batch has > 16 limb columns
+  int wide;            // 1 wide scan units where possible, 0 never, -1 for databases of several record chunks
+  int bn_cap;          // largest limb-column tile of the pair kernels (32..256), 0 = 256
+  int units_per_pair;  // scan split target: units per resident CTA pair, 0 = 12
 };
 
 struct Engine {
@@ -151,7 +175,50 @@ struct Engine {
   long long kernel_batches = 0;
   CUtensorMap map_db, map_ub;
   int last_launches = 0;
+  bool use_graphs = false;  // replay captured launch sequences (alto_engine_set_graphs)
+  std::vector<TuneEntry> tuning;  // sorted by b_max; the first entry with b_max >= batch size applies
 };
+
+const TuneEntry *tune_for(const Engine *e, size_t slots) {
+  for (const TuneEntry &t : e->tuning)
+    if ((size_t)t.b_max >= slots) return &t;
+  return nullptr;
+}
+
+// The committed tuning table: lines "rows_max b_max pair wide bn_cap units_per_pair" ('#' starts a comment); the
+// rows of the smallest rows_max >= the engine's record count apply.  Read from $ALTO_TUNING, else from tuning.txt
+// next to this library.
+void load_tuning(Engine *e) {
+  std::string path;
+  if (const char *env = getenv("ALTO_TUNING")) {
+    path = env;
+  } else {
+    Dl_info info;
+    if (dladdr(reinterpret_cast<void *>(&load_tuning), &info) && info.dli_fname) {
+      path = info.dli_fname;
+      const size_t slash = path.find_last_of('/');
+      path = (slash == std::string::npos ? std::string() : path.substr(0, slash + 1)) + "tuning.txt";
+    }
+  }
+  FILE *f = path.empty() ? nullptr : fopen(path.c_str(), "r");
+  if (!f) return;
+  std::vector<std::pair<long long, TuneEntry>> rows;
+  char line[256];
+  while (fgets(line, sizeof line, f)) {
+    if (line[0] == '#') continue;
+    long long rmax;
+    TuneEntry t;
+    if (sscanf(line, "%lld %d %d %d %d %d", &rmax, &t.b_max, &t.pair, &t.wide, &t.bn_cap, &t.units_per_pair) == 6)
+      rows.push_back({rmax, t});
+  }
+  fclose(f);
+  long long best = -1;
+  for (auto &r : rows)
+    if (r.first >= (long long)e->rows && (best < 0 || r.first < best)) best = r.first;
+  for (auto &r : rows)
+    if (r.first == best) e->tuning.push_back(r.second);
+  std::sort(e->tuning.begin(), e->tuning.end(), [](const TuneEntry &a, const TuneEntry &b) { return a.b_max < b.b_max; });
+}
 
 // Adds the kernel intervals of one recorded timing set to the engine's totals (its last mark must have completed).
 bool accumulate(Engine *e, int set) {
@@ -189,6 +256,7 @@ bool next_set(Engine *e, int *set) {
 }
 
 void free_scratch(Batch *b) {
+  clear_graphs(b);  // graphs hold the scratch addresses
   cudaFree(b->d_req);
   cudaFree(b->d_qlimb);
   cudaFree(b->d_ylimb);
@@ -366,7 +434,9 @@ bool pair_kernels_enabled() {
 Plan make_plan(const Engine *e, size_t slots) {
   Plan p;
   const size_t limb_cols = 4 * round_up(slots, 4);
+  const TuneEntry *tn = tune_for(e, slots);
   p.pair = limb_cols > 16 && pair_kernels_enabled();
+  if (tn && tn->pair >= 0) p.pair = tn->pair == 1 && limb_cols > 16 && pair_kernels_enabled();
   p.scan_kb = (int)((e->rows + alto::kBK - 1) / alto::kBK);
   p.pack_kb = (int)(e->count / alto::kBK);
   // with several record chunks a unit must stay inside one: its length divides the 256 blocks of a chunk
@@ -392,8 +462,9 @@ Plan make_plan(const Engine *e, size_t slots) {
     p.scan_split = (p.scan_kb + p.scan_kb_per - 1) / p.scan_kb_per;
     return p;
   }
+  const int bn_cap = (tn && tn->bn_cap >= 32 && tn->bn_cap <= 256) ? tn->bn_cap : 256;
   p.bn = 32;
-  while (p.bn < 256 && (size_t)p.bn < limb_cols) p.bn *= 2;
+  while (p.bn < bn_cap && (size_t)p.bn < limb_cols) p.bn *= 2;
   p.num_n = (int)((limb_cols + p.bn - 1) / p.bn);
   p.scan_m = (int)((e->cols + 255) / 256);
   p.pack_m = (int)((4 * e->cols + 255) / 256);
@@ -401,12 +472,14 @@ Plan make_plan(const Engine *e, size_t slots) {
   // Wide scan units once the database spans several record chunks (its tiles then stream from HBM and cannot be
   // shared between two pairs through L2) and there are at least 512 limb columns; ALTO_SCAN_WIDE=0/1 overrides.
   p.wide = p.bn == 256 && p.num_n >= 2 && e->nchunks > 1;
+  if (tn && tn->wide >= 0) p.wide = p.bn == 256 && p.num_n >= 2 && tn->wide == 1;
   if (const char *w = getenv("ALTO_SCAN_WIDE")) p.wide = p.bn == 256 && p.num_n >= 2 && w[0] == '1';
   p.scan_n = p.wide ? (p.num_n + 1) / 2 : p.num_n;
   // Scan chunks: at most 256 blocks (exactness, as above), at least 8, and about twelve units per resident pair so
   // the persistent pairs finish together.
   const long tiles = (long)p.scan_m * p.scan_n;
-  long split = std::max<long>((p.scan_kb + 255) / 256, (12L * pairs + tiles - 1) / tiles);
+  const long upp = (tn && tn->units_per_pair > 0) ? tn->units_per_pair : 12;
+  long split = std::max<long>((p.scan_kb + 255) / 256, (upp * pairs + tiles - 1) / tiles);
   split = std::min<long>(split, std::max<long>(1, p.scan_kb / 8));
   split = std::max<long>(split, (p.scan_kb + 255) / 256);
   p.scan_kb_per = chunk_aligned((int)((p.scan_kb + split - 1) / split));
@@ -501,8 +574,9 @@ bool make_limb_maps(const Engine *e, const Plan &p, const uint8_t *qlimb, const 
 // scan GEMM and tail.  The pack needs only the keys, so it overlaps the upload of the much larger query words.
 // Statuses go to d_status (and to the pinned host copy when host_status); responses of valid frames to
 // resp + slot * resp_stride.
-bool enqueue_batch(Engine *e, Batch *bt, const uint8_t *d_slots, size_t slot_stride, size_t slots, uint8_t *resp,
-                   size_t resp_stride, bool host_status, cudaEvent_t queries_ready = nullptr) {
+bool enqueue_batch_direct(Engine *e, Batch *bt, const uint8_t *d_slots, size_t slot_stride, size_t slots,
+                          uint8_t *resp, size_t resp_stride, bool host_status, cudaEvent_t queries_ready,
+                          bool with_marks) {
   cudaStream_t st = bt->st;
   const Plan p = make_plan(e, slots);
   const int bp = (int)round_up(slots, 4);
@@ -510,7 +584,7 @@ bool enqueue_batch(Engine *e, Batch *bt, const uint8_t *d_slots, size_t slot_str
   // timing marks (main batch only): 0 begin | validate | 1 | y split | 2 | pack | 3 | (query wait) q split,
   // zeroing | 4 | scan | 5 | tail | 6
   cudaEvent_t *mk = nullptr;
-  if (bt->timing) {
+  if (bt->timing && with_marks) {
     int set = 0;
     if (!next_set(e, &set)) return false;
     mk = e->marks[set];
@@ -578,6 +652,43 @@ bool enqueue_batch(Engine *e, Batch *bt, const uint8_t *d_slots, size_t slot_str
   }
   ALTO_CK(mark(6));
   e->last_launches = launches;
+  return true;
+}
+
+// enqueue_batch_direct, or -- when the engine replays graphs and the batch does not wait on another stream -- the
+// same sequence as a CUDA graph captured on first use for this batch size and these buffers and replayed after.
+// Graph replays record no per-kernel timing marks.
+bool enqueue_batch(Engine *e, Batch *bt, const uint8_t *d_slots, size_t slot_stride, size_t slots, uint8_t *resp,
+                   size_t resp_stride, bool host_status, cudaEvent_t queries_ready = nullptr) {
+  if (!e->use_graphs || queries_ready)
+    return enqueue_batch_direct(e, bt, d_slots, slot_stride, slots, resp, resp_stride, host_status, queries_ready,
+                                true);
+  for (const Batch::GraphEntry &g : bt->graphs)
+    if (g.slots == slots && g.d_slots == d_slots && g.stride == slot_stride && g.resp == resp &&
+        g.resp_stride == resp_stride && g.host_status == host_status) {
+      ALTO_CK(cudaGraphLaunch(g.exec, bt->st));
+      return true;
+    }
+  ALTO_CK(cudaStreamBeginCapture(bt->st, cudaStreamCaptureModeThreadLocal));
+  const bool ok =
+      enqueue_batch_direct(e, bt, d_slots, slot_stride, slots, resp, resp_stride, host_status, nullptr, false);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t end = cudaStreamEndCapture(bt->st, &graph);
+  if (!ok || end != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    if (ok) set_error("graph capture", end);
+    return false;
+  }
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t inst = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  ALTO_CK(inst);
+  if (bt->graphs.size() >= 64) {  // bounded cache: drop the oldest graph
+    cudaGraphExecDestroy(bt->graphs.front().exec);
+    bt->graphs.erase(bt->graphs.begin());
+  }
+  bt->graphs.push_back({slots, slot_stride, resp_stride, d_slots, resp, host_status, exec});
+  ALTO_CK(cudaGraphLaunch(exec, bt->st));
   return true;
 }
 
@@ -830,6 +941,8 @@ void *alto_engine_new(const uint8_t *db_col, const uint8_t *db_tiled, size_t ld,
     destroy(e);
     return nullptr;
   }
+  resident_pairs();  // occupancy query outside any stream capture
+  load_tuning(e);
   return e;
 }
 
@@ -917,6 +1030,28 @@ int alto_kernel_times(void *p, double *ms, long long *batches, int reset) {
 }
 
 int alto_last_launches(const void *p) { return p ? static_cast<const Engine *>(p)->last_launches : 0; }
+
+int alto_engine_set_tuning(void *p, const int32_t *entries, size_t n) {
+  Engine *e = static_cast<Engine *>(p);
+  if (!e || (n && !entries)) return -1;
+  if (cudaSetDevice(e->dev) != cudaSuccess || cudaStreamSynchronize(e->main.st) != cudaSuccess) return -4;
+  e->tuning.clear();
+  for (size_t i = 0; i < n; ++i)
+    e->tuning.push_back({entries[5 * i], entries[5 * i + 1], entries[5 * i + 2], entries[5 * i + 3],
+                         entries[5 * i + 4]});
+  std::sort(e->tuning.begin(), e->tuning.end(), [](const TuneEntry &a, const TuneEntry &b) { return a.b_max < b.b_max; });
+  clear_graphs(&e->main);  // captured sequences follow the old plans
+  return 0;
+}
+
+int alto_engine_set_graphs(void *p, int on) {
+  Engine *e = static_cast<Engine *>(p);
+  if (!e) return -1;
+  if (cudaSetDevice(e->dev) != cudaSuccess || cudaStreamSynchronize(e->main.st) != cudaSuccess) return -4;
+  e->use_graphs = on != 0;
+  if (!e->use_graphs) clear_graphs(&e->main);
+  return 0;
+}
 
 int alto_synthetic_db_col_device(uint8_t *d_db, size_t ld, size_t rows, size_t col0, size_t ncols) {
   if (rows % 4 || ld % 4) return -1;

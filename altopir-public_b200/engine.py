@@ -154,6 +154,18 @@ class Engine:
             raise EngineError(f"engine error {r}: {last_error()}")
         return list(ms), nb.value
 
+    def set_tuning(self, entries):
+        """alto_engine_set_tuning: entries = [(b_max, pair, wide, bn_cap, units_per_pair), ...]; [] clears."""
+        arr = np.ascontiguousarray(np.array(entries, dtype=np.int32).reshape(-1))
+        if lib().alto_engine_set_tuning(self.ptr, ctypes.c_void_p(arr.ctypes.data) if arr.size else None,
+                                        len(entries)) < 0:
+            raise EngineError(last_error())
+
+    def set_graphs(self, on=True):
+        """alto_engine_set_graphs: replay captured CUDA graphs for device-resident batches."""
+        if lib().alto_engine_set_graphs(self.ptr, int(on)) < 0:
+            raise EngineError(last_error())
+
     def last_launches(self):
         return lib().alto_last_launches(self.ptr)
 

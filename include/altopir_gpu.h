@@ -112,6 +112,22 @@ int alto_engine_sync(void *engine);
 /* The cudaStream_t the engine launches its kernels on (for events and stream ordering in the caller). */
 void *alto_engine_stream(void *engine);
 
+/* Tuning table of this engine: n entries of 5 ints {b_max, pair, wide, bn_cap, units_per_pair}; the first entry
+ * (in b_max order) with b_max >= the batch size chooses the GEMM plan: pair = 1 CTA-pair kernels, 0 single-CTA
+ * kernels; wide = 1 scan units of 512 limb columns, 0 never; bn_cap = largest limb-column tile (32..256);
+ * units_per_pair = scan split target; -1 or 0 keeps the built-in choice.  Every plan computes identical results.
+ * alto_engine_new loads the committed table from $ALTO_TUNING or tuning.txt next to this library (lines
+ * "rows_max b_max pair wide bn_cap units_per_pair", the rows of the smallest rows_max >= the engine's records).
+ * n = 0 clears the table.  Returns 0, -1 for bad arguments, -4 on a device failure. */
+int alto_engine_set_tuning(void *engine, const int32_t *entries, size_t n);
+
+/* Replay the device-side launch sequence of a batch (validate .. tail) as a CUDA graph, captured on the first batch
+ * of each size and buffer set (on = 1), or launch kernels directly (on = 0, the default).  Applies to
+ * alto_answer_device, alto_enqueue_device and serving loops created afterwards; alto_answer keeps direct launches
+ * because its pack overlaps the query upload on another stream.  Graph replays record no timing marks for
+ * alto_kernel_times.  Returns 0, or -4 on a device failure. */
+int alto_engine_set_graphs(void *engine, int on);
+
 /* Device time in ms summed over the batches since the last reset, measured with CUDA events on the engine's
  * stream: ms[0] validate, ms[1] limb split + accumulator zeroing, ms[2] scan GEMM, ms[3] pack GEMM, ms[4] tail;
  * *batches receives the number of batches.  Synchronises the engine.  Returns 0, or -4 on a device failure. */

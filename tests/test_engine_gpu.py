@@ -166,3 +166,39 @@ def test_1gb_batch_128_sampled_parts_match_oracle(gpu, oracle, svc, eng):
         assert rr == b and np.array_equal(rout, out)
         ref.close()
     e.close()
+
+
+def test_every_plan_and_the_graph_path_return_identical_bytes(gpu, svc, eng):
+    import torch
+    p = svc.params(2048, 4096)
+    st = svc.SyntheticState.make(p, seed=27)
+    e = eng.Engine.from_state(st)
+    b = 136
+    frames = svc.synthetic_requests(p, b, seed=28)
+    ql, rl = e.request_len(), e.response_len()
+    stride = (7 + ql + 15) // 16 * 16
+    slots = torch.zeros((b, stride), dtype=torch.uint8, device="cuda")
+    slots[:, 7:7 + ql] = torch.from_numpy(frames).cuda()
+    status = np.full(b, -1, dtype=np.int32)
+
+    def run():
+        out = torch.zeros((b, rl), dtype=torch.uint8, device="cuda")
+        assert e.answer_device(slots.data_ptr(), stride, b, out.data_ptr(), rl, status) == b
+        return out.cpu().numpy()
+
+    want = run()
+    plans = [(b, 0, -1, 0, 0), (b, 1, 0, 64, 4), (b, 1, 0, 128, 24), (b, 1, 1, 256, 12), (b, 1, 0, 32, 6)]
+    for plan in plans:
+        e.set_tuning([plan])
+        assert np.array_equal(run(), want), plan
+    e.set_tuning([])
+    e.set_graphs(True)
+    for _ in range(3):  # capture on the first call, replay after
+        assert np.array_equal(run(), want)
+    for bb in (1, 5, 136):
+        out = torch.zeros((bb, rl), dtype=torch.uint8, device="cuda")
+        e.enqueue_device(slots.data_ptr(), stride, bb, out.data_ptr(), rl)
+        e.sync()
+        assert np.array_equal(out.cpu().numpy(), want[:bb]), bb
+    e.set_graphs(False)
+    e.close()
