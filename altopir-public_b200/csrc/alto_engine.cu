@@ -167,6 +167,8 @@ struct Engine {
   // per call: before the uploads, after the downloads; the query words upload on st_copy
   cudaEvent_t ev_begin = nullptr, ev_end = nullptr, ev_keys = nullptr, ev_queries = nullptr;
   cudaStream_t st_copy = nullptr;
+  // host pipeline of alto_answer: keys uploaded, pack done, statuses ready, each column group's tail done
+  cudaEvent_t ev_pack = nullptr, ev_status = nullptr, ev_group[8] = {};
   // per batch: a ring of kMarks timing marks, accumulated into kernel_ms when the stream is synchronised
   cudaEvent_t marks[kTimingSets][kMarks] = {};
   int mark_next = 0, last_set = 0;
@@ -302,7 +304,9 @@ void destroy(Engine *e) {
   cudaFree(e->d_that);
   cudaFree(e->d_tw);
   if (e->st_copy) cudaStreamSynchronize(e->st_copy);
-  for (cudaEvent_t ev : {e->ev_begin, e->ev_end, e->ev_keys, e->ev_queries})
+  for (cudaEvent_t ev : {e->ev_begin, e->ev_end, e->ev_keys, e->ev_queries, e->ev_pack, e->ev_status})
+    if (ev) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : e->ev_group)
     if (ev) cudaEventDestroy(ev);
   if (e->st_copy) cudaStreamDestroy(e->st_copy);
   for (auto &set : e->marks)
@@ -491,15 +495,18 @@ Plan make_plan(const Engine *e, size_t slots) {
 
 // The scan GEMM (acc sums, pre-zeroed) and the pack GEMM (beta) for `slots` clients under plan p.
 bool launch_scan(const Engine *e, const Plan &p, const CUtensorMap &map_q, uint32_t *acc, size_t slots,
-                 cudaStream_t st, uint32_t *err) {
+                 cudaStream_t st, uint32_t *err, int group = 0, int groups = 1) {
+  // column group `group` of `groups`: scan tiles [m0, m0 + mg) (the plan's tile count divides by the groups)
+  const int mg = p.scan_m / groups, m0 = group * mg;
   // The query limbs are re-read by every unit of a K chunk; mark them evict-last only while the whole operand
   // (4 bytes per record and client) is a small part of the 126 MB L2, so stale chunks never crowd it out.
   const int keep_b = 4 * round_up(slots, 4) * e->rows <= (size_t(32) << 20);
   if (p.pair) {
     alto::PairArgs g;
-    g.num_m = p.scan_m;
+    g.num_m = mg;
+    g.m_begin = m0;
     g.num_n = p.scan_n;
-    g.num_units = p.scan_m * p.scan_n * p.scan_split;
+    g.num_units = mg * p.scan_n * p.scan_split;
     g.kb_total = p.scan_kb;
     g.kb_per_unit = p.scan_kb_per;
     g.rows_a = (int)e->cols;
@@ -509,10 +516,12 @@ bool launch_scan(const Engine *e, const Plan &p, const CUtensorMap &map_q, uint3
     g.err = err;
     g.b_keep = keep_b;
     g.kb_chunk = p.kb_chunk;
-    return dispatch_pair<alto::Epi::kScan>(p.bn, e->map_db, map_q, g, p.pairs_scan, st, p.wide);
+    return dispatch_pair<alto::Epi::kScan>(p.bn, e->map_db, map_q, g,
+                                           std::min(p.pairs_scan, g.num_units), st, p.wide);
   }
   alto::GemmArgs g;
-  g.num_m = p.scan_m;
+  g.num_m = mg;
+  g.m_begin = m0;
   g.num_n = p.num_n;
   g.kb_total = p.scan_kb;
   g.kb_per_unit = p.scan_kb_per;
@@ -523,7 +532,7 @@ bool launch_scan(const Engine *e, const Plan &p, const CUtensorMap &map_q, uint3
   g.err = err;
   g.b_keep = keep_b;
   g.kb_chunk = p.kb_chunk;
-  return dispatch_gemm<alto::Epi::kScan>(p.bn, e->map_db, map_q, g, p.scan_m * p.num_n * p.scan_split, st);
+  return dispatch_gemm<alto::Epi::kScan>(p.bn, e->map_db, map_q, g, mg * p.num_n * p.scan_split, st);
 }
 
 bool launch_pack(const Engine *e, const Plan &p, const CUtensorMap &map_y, uint32_t *beta, size_t slots,
@@ -532,6 +541,7 @@ bool launch_pack(const Engine *e, const Plan &p, const CUtensorMap &map_y, uint3
   if (p.pair) {
     alto::PairArgs g;
     g.num_m = p.pack_m;
+    g.m_begin = 0;
     g.num_n = p.num_n;
     g.num_units = p.pack_m * p.num_n;
     g.kb_total = p.pack_kb;
@@ -547,6 +557,7 @@ bool launch_pack(const Engine *e, const Plan &p, const CUtensorMap &map_y, uint3
   }
   alto::GemmArgs g;
   g.num_m = p.pack_m;
+  g.m_begin = 0;
   g.num_n = p.num_n;
   g.kb_total = p.pack_kb;
   g.kb_per_unit = p.pack_kb;
@@ -647,6 +658,8 @@ bool enqueue_batch_direct(Engine *e, Batch *bt, const uint8_t *d_slots, size_t s
     t.row1_off = (int)e->row1_off;
     t.q1_bits = e->q1_bits;
     t.q1 = (int64_t)e->q1;
+    t.o_begin = 0;
+    t.o_count = (int)e->outputs;
     ALTO_CK(alto::launch_tail(t, slots, st));
     ++launches;
   }
@@ -771,6 +784,19 @@ bool host_header_status(const Engine *e, const uint8_t *f, size_t len, int *stat
   return true;
 }
 
+// Column groups of the host pipeline: whole response parts per group, an integral number of scan tiles each.
+// ALTO_HOST_GROUPS (1, 2, 4 or 8) overrides the default of two.
+int host_groups(const Engine *e, const Plan &p) {
+  int want = 2;
+  if (const char *v = getenv("ALTO_HOST_GROUPS")) want = std::max(1, std::min(8, atoi(v)));
+  for (int g = want; g > 1; g /= 2)
+    if (e->outputs % g == 0 && p.scan_m % g == 0) return g;
+  return 1;
+}
+
+// alto_answer: header and y keys upload first and the pack starts on them while z keys and query words upload on
+// the copy stream; then validation, the query limb split, and the scan and tail in column groups.  The responses of
+// a group download (valid frames only, on the copy stream) while the next group computes.
 int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t b, uint8_t *const *out, int *status,
                 double *stage_ms) {
   std::vector<size_t> cand;
@@ -794,40 +820,127 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
     return -3;
   }
   if (cudaSetDevice(e->dev) != cudaSuccess || !ensure_capacity(e, &e->main, cand.size())) return -4;
-  cudaStream_t st = e->main.st;
-  if (cudaEventRecord(e->ev_begin, st) != cudaSuccess) return -4;
-  // header and keys first on the compute stream, then the query words on the copy stream, so that validation and
-  // the pack run while the queries are still uploading
-  const size_t head = 9 + 8 * e->count;
+  Batch *bt = &e->main;
+  cudaStream_t st = bt->st, sc = e->st_copy;
+  const size_t nc = cand.size();
+  const Plan p = make_plan(e, nc);
+  const int groups = host_groups(e, p);
+  const int bp = (int)round_up(nc, 4);
+  const size_t ybytes = 9 + 4 * e->count;  // header and y keys
+  int launches = 0;
+#define ALTO_H(call)                   \
+  do {                                 \
+    cudaError_t e_ = (call);           \
+    if (e_ != cudaSuccess) {           \
+      set_error(#call, e_);            \
+      return -4;                       \
+    }                                  \
+  } while (0)
+  ALTO_H(cudaEventRecord(e->ev_begin, st));
   if (!copy_runs(
-          cand.size(), head, [&](size_t i) { return (const void *)req[cand[i]]; },
-          [&](size_t i) { return (void *)(e->main.d_req + i * e->slot_stride + kSlotLead); }, cudaMemcpyHostToDevice, st))
+          nc, ybytes, [&](size_t i) { return (const void *)req[cand[i]]; },
+          [&](size_t i) { return (void *)(bt->d_req + i * e->slot_stride + kSlotLead); }, cudaMemcpyHostToDevice, st))
     return -4;
-  if (cudaEventRecord(e->ev_keys, st) != cudaSuccess || cudaStreamWaitEvent(e->st_copy, e->ev_keys, 0) != cudaSuccess)
-    return -4;
+  ALTO_H(cudaEventRecord(e->ev_keys, st));
+  ALTO_H(cudaStreamWaitEvent(sc, e->ev_keys, 0));
   if (!copy_runs(
-          cand.size(), e->want - head, [&](size_t i) { return (const void *)(req[cand[i]] + head); },
-          [&](size_t i) { return (void *)(e->main.d_req + i * e->slot_stride + kSlotLead + head); },
-          cudaMemcpyHostToDevice, e->st_copy))
+          nc, e->want - ybytes, [&](size_t i) { return (const void *)(req[cand[i]] + ybytes); },
+          [&](size_t i) { return (void *)(bt->d_req + i * e->slot_stride + kSlotLead + ybytes); },
+          cudaMemcpyHostToDevice, sc))
     return -4;
-  if (cudaEventRecord(e->ev_queries, e->st_copy) != cudaSuccess) return -4;
-  if (!enqueue_batch(e, &e->main, e->main.d_req, e->slot_stride, cand.size(), e->main.d_resp, e->resp_len, true, e->ev_queries))
-    return -4;
-  if (cudaEventSynchronize(e->marks[e->last_set][1]) != cudaSuccess) {
-    set_error("status event failed");
-    return -4;
+  ALTO_H(cudaEventRecord(e->ev_queries, sc));
+
+  CUtensorMap map_q, map_y;
+  if (!make_limb_maps(e, p, bt->d_qlimb, bt->d_ylimb, bp, &map_q, &map_y)) return -4;
+  const unsigned tpb = 256;
+  {
+    const size_t work = (e->count / 16) * (size_t)bp;
+    alto::limb_split_kernel<<<(unsigned)((work + tpb - 1) / tpb), tpb, 0, st>>>(
+        bt->d_req, e->slot_stride, kSlotLead + 9, (int)nc, bp, e->count, e->count, bt->d_ylimb);
+    ALTO_H(cudaGetLastError());
+    ++launches;
   }
+  if (!launch_pack(e, p, map_y, bt->d_beta, nc, st, bt->d_err)) return -4;
+  ++launches;
+  ALTO_H(cudaEventRecord(e->ev_pack, st));
+  ALTO_H(cudaStreamWaitEvent(st, e->ev_queries, 0));
+  alto::validate_kernel<<<(unsigned)nc, 256, 0, st>>>(bt->d_req, e->slot_stride, kSlotLead, e->count, e->rows,
+                                                      bt->d_status);
+  ALTO_H(cudaGetLastError());
+  ++launches;
+  ALTO_H(cudaMemcpyAsync(bt->h_status, bt->d_status, nc * sizeof(int), cudaMemcpyDeviceToHost, st));
+  ALTO_H(cudaEventRecord(e->ev_status, st));
+  {
+    const size_t work = (e->rows / 16) * (size_t)bp;
+    alto::limb_split_kernel<<<(unsigned)((work + tpb - 1) / tpb), tpb, 0, st>>>(
+        bt->d_req, e->slot_stride, kSlotLead + 9 + 8 * e->count, (int)nc, bp, e->rows, e->chunk, bt->d_qlimb);
+    ALTO_H(cudaGetLastError());
+    ++launches;
+  }
+  ALTO_H(cudaMemsetAsync(bt->d_acc, 0, nc * e->cols * sizeof(uint32_t), st));
+  const int parts = (int)e->outputs / groups;
+  for (int g = 0; g < groups; ++g) {
+    if (!launch_scan(e, p, map_q, bt->d_acc, nc, st, bt->d_err, g, groups)) return -4;
+    alto::TailArgs t;
+    t.acc = bt->d_acc;
+    t.beta = bt->d_beta;
+    t.status = bt->d_status;
+    t.req = bt->d_req;
+    t.req_stride = e->slot_stride;
+    t.z_off = kSlotLead + 9 + 4 * e->count;
+    t.that = e->d_that;
+    t.twiddle = e->d_tw;
+    t.prefix = e->d_prefix;
+    t.resp = bt->d_resp;
+    t.resp_stride = e->resp_len;
+    t.n = (int)e->n;
+    t.tg = (int)e->tg;
+    t.outputs = (int)e->outputs;
+    t.cols = (int)e->cols;
+    t.part_len = (int)e->part_len;
+    t.row1_off = (int)e->row1_off;
+    t.q1_bits = e->q1_bits;
+    t.q1 = (int64_t)e->q1;
+    t.o_begin = g * parts;
+    t.o_count = parts;
+    ALTO_H(alto::launch_tail(t, nc, st));
+    launches += 2;
+    ALTO_H(cudaEventRecord(e->ev_group[g], st));
+  }
+  e->last_launches = launches;
+
+  // statuses come back as soon as validation is done; then each group's valid responses download on the copy
+  // stream behind that group's tail
+  ALTO_H(cudaEventSynchronize(e->ev_status));
   std::vector<size_t> ok;  // indices into cand with status 0
-  for (size_t i = 0; i < cand.size(); ++i) {
-    status[cand[i]] = e->main.h_status[i];
-    if (e->main.h_status[i] == 0) ok.push_back(i);
+  for (size_t i = 0; i < nc; ++i) {
+    status[cand[i]] = bt->h_status[i];
+    if (bt->h_status[i] == 0) ok.push_back(i);
   }
-  if (!copy_runs(
-          ok.size(), e->resp_len, [&](size_t k) { return (const void *)(e->main.d_resp + ok[k] * e->resp_len); },
-          [&](size_t k) { return (void *)out[cand[ok[k]]]; }, cudaMemcpyDeviceToHost, st))
-    return -4;
-  if (cudaEventRecord(e->ev_end, st) != cudaSuccess) return -4;
-  if (!finish(e, stage_ms)) return -4;
+  const size_t gbytes = (size_t)parts * e->part_len;
+  for (int g = 0; g < groups; ++g) {
+    ALTO_H(cudaStreamWaitEvent(sc, e->ev_group[g], 0));
+    const size_t off = (size_t)g * gbytes;
+    if (!copy_runs(
+            ok.size(), gbytes, [&](size_t k) { return (const void *)(bt->d_resp + ok[k] * e->resp_len + off); },
+            [&](size_t k) { return (void *)(out[cand[ok[k]]] + off); }, cudaMemcpyDeviceToHost, sc))
+      return -4;
+  }
+  ALTO_H(cudaEventRecord(e->ev_end, sc));
+  ALTO_H(cudaStreamSynchronize(sc));
+  if (!sync_engine(e)) return -4;
+  if (stage_ms) {
+    float t0, t1, t2, t3;
+    ALTO_H(cudaEventElapsedTime(&t0, e->ev_begin, e->ev_keys));                // key upload
+    ALTO_H(cudaEventElapsedTime(&t1, e->ev_status, e->ev_group[groups - 1]));  // query split + scan + tails
+    ALTO_H(cudaEventElapsedTime(&t2, e->ev_keys, e->ev_pack));                 // key split + pack
+    ALTO_H(cudaEventElapsedTime(&t3, e->ev_group[groups - 1], e->ev_end));     // last download
+    stage_ms[0] = t0;
+    stage_ms[1] = t1;
+    stage_ms[2] = t2;
+    stage_ms[3] = t3;
+  }
+#undef ALTO_H
   return (int)ok.size();
 }
 
@@ -897,8 +1010,11 @@ void *alto_engine_new(const uint8_t *db_col, const uint8_t *db_tiled, size_t ld,
   if ((err = cudaStreamCreateWithFlags(&e->st_copy, cudaStreamNonBlocking)) != cudaSuccess) return fail("stream", err);
   if ((err = cudaEventCreate(&e->ev_begin)) != cudaSuccess || (err = cudaEventCreate(&e->ev_end)) != cudaSuccess ||
       (err = cudaEventCreateWithFlags(&e->ev_keys, cudaEventDisableTiming)) != cudaSuccess ||
-      (err = cudaEventCreateWithFlags(&e->ev_queries, cudaEventDisableTiming)) != cudaSuccess)
+      (err = cudaEventCreateWithFlags(&e->ev_queries, cudaEventDisableTiming)) != cudaSuccess ||
+      (err = cudaEventCreate(&e->ev_pack)) != cudaSuccess || (err = cudaEventCreate(&e->ev_status)) != cudaSuccess)
     return fail("event", err);
+  for (cudaEvent_t &ev : e->ev_group)
+    if ((err = cudaEventCreate(&ev)) != cudaSuccess) return fail("event", err);
   for (auto &set : e->marks)
     for (cudaEvent_t &ev : set)
       if ((err = cudaEventCreate(&ev)) != cudaSuccess) return fail("event", err);
@@ -1178,6 +1294,8 @@ bool enqueue_noalloc(Engine *e, uint8_t *scratch, const NoAllocLayout &l, const 
   t.row1_off = (int)e->row1_off;
   t.q1_bits = e->q1_bits;
   t.q1 = (int64_t)e->q1;
+  t.o_begin = 0;
+  t.o_count = (int)e->outputs;
   ALTO_CK(alto::launch_tail(t, b, st));
   ALTO_CK(cudaMemcpyAsync(d_status, status, b * sizeof(int), cudaMemcpyDeviceToDevice, st));
   return true;

@@ -91,6 +91,7 @@ struct TailArgs {
   int n, tg, outputs, cols;
   int part_len, row1_off, q1_bits;
   int64_t q1;
+  int o_begin, o_count;     // this launch answers parts o_begin .. o_begin + o_count of every slot
 };
 
 // One response part per CTA (slot, output o), n / 8 threads owning 8 coefficients each.
@@ -130,7 +131,7 @@ template <int L>
 __global__ void __launch_bounds__((1 << L) / 8) tail_kernel(TailArgs a) {
   constexpr int n = 1 << L, NT = n / 8;
   extern __shared__ uint32_t tsm[];
-  const int slot = blockIdx.x / a.outputs, o = blockIdx.x % a.outputs;
+  const int slot = blockIdx.x / a.o_count, o = a.o_begin + blockIdx.x % a.o_count;
   if (a.status[slot] != 0) return;  // rejected frames get no response (their output stays untouched)
   const int tid = threadIdx.x;
   uint32_t *acc = tsm;
@@ -234,7 +235,7 @@ __global__ void __launch_bounds__((1 << L) / 8) tail_kernel(TailArgs a) {
 // The same computation for small rings (n < 256), one coefficient pair per thread and stage.
 __global__ void __launch_bounds__(128) tail_small_kernel(TailArgs a) {
   extern __shared__ uint32_t tsm[];
-  const int slot = blockIdx.x / a.outputs, o = blockIdx.x % a.outputs;
+  const int slot = blockIdx.x / a.o_count, o = a.o_begin + blockIdx.x % a.o_count;
   if (a.status[slot] != 0) return;
   const int n = a.n, tid = threadIdx.x, nt = blockDim.x;
   uint32_t *acc = tsm;
@@ -316,7 +317,7 @@ namespace alto {
 // Launches the tail for `slots` frames on stream st: the radix-8 kernel for n >= 256, the simple one below.
 inline cudaError_t launch_tail(const TailArgs &t, size_t slots, cudaStream_t st) {
   const size_t smem = ((size_t)t.n + (t.part_len + 3) / 4 + 1) * sizeof(uint32_t);
-  const unsigned grid = (unsigned)(slots * t.outputs);
+  const unsigned grid = (unsigned)(slots * t.o_count);
   cudaError_t err = cudaSuccess;
   auto go = [&](auto kernel, unsigned threads) {
     if (smem > 48 * 1024) err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -37,6 +37,7 @@ struct GemmArgs {
   uint32_t *err;    // device error word
   int b_keep;       // 1: keep the B operand in L2 (evict_last; it is small and read by every unit), 0: normal
   int kb_chunk;     // scan: 128-byte blocks per record chunk of the 3-D operand maps (units never straddle chunks)
+  int m_begin;      // first tile along A (a launch may cover a column group: tiles m_begin .. m_begin + num_m)
 };
 
 // x mod Q for any 64-bit x, using 2^32 = 12287 (mod Q): two folds leave x < 2^32 + 2^28, one subtraction finishes.
@@ -78,7 +79,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int u = blockIdx.x;
   const int n_tile = u % args.num_n;
-  const int m_tile = (u / args.num_n) % args.num_m;
+  const int m_tile = args.m_begin + (u / args.num_n) % args.num_m;
   const int k_chunk = u / (args.num_n * args.num_m);
   const int kb0 = k_chunk * args.kb_per_unit;
   const int kb1 = min(kb0 + args.kb_per_unit, args.kb_total);

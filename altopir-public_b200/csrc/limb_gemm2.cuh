@@ -53,6 +53,7 @@ struct PairArgs {
   uint32_t *err;    // device error word
   int b_keep;       // 1: keep the B operand in L2 (evict_last; it is small and read by every unit), 0: normal
   int kb_chunk;     // scan: 128-byte blocks per record chunk of the 3-D operand maps (units never straddle chunks)
+  int m_begin;      // first 256-row tile along A (a launch may cover a column group)
 };
 
 // Epilogue of 16 TMEM columns (4 clients x 4 limbs) for one accumulator row of the scan: row = database column.
@@ -138,7 +139,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
 
   auto unit_coords = [&](int u, int &m, int &n, int &kb0, int &nkb) {
     n = u % args.num_n;
-    m = (u / args.num_n) % args.num_m;
+    m = args.m_begin + (u / args.num_n) % args.num_m;
     const int kc = u / (args.num_n * args.num_m);
     kb0 = kc * args.kb_per_unit;
     nkb = min(kb0 + args.kb_per_unit, args.kb_total) - kb0;

@@ -72,9 +72,11 @@ size_t alto_response_len(const void *engine);
  *   status[c] = 1 for a NULL frame or a length other than alto_request_len, 2 for a flag byte != 0 or a key count
  *   != tg * n, 3 for a y or z key word >= q, else 0 (query words are not range-checked);
  *   out[c] (alto_response_len bytes) is written for status 0 only, other output buffers stay untouched.
- * method must be 0 (the reference's AMX code) or 2 (VNNI); both run the same GPU path.  When stage_ms is not NULL
- * it receives device times in ms of the reference's four stages: [0] key upload + validation, [1] scan (including
- * any wait for the query upload, which overlaps the pack), [2] pack, [3] tail + download.
+ * method must be 0 (the reference's AMX code) or 2 (VNNI); both run the same GPU path.  The header and y keys upload
+ * first and the pack runs while the z keys and query words upload; the scan and tail then run in column groups
+ * whose responses download while the next group computes.  When stage_ms is not NULL it receives device times in
+ * ms: [0] header and y-key upload, [1] validation, query split, scans and tails, [2] key split and pack, [3] the
+ * last group's download.
  * Returns the number of valid requests, -1 for bad arguments, -3 when the tail parameters are invalid (n not a
  * power of two >= 16, q1 >= 2^21, q1_bits > 24, n % 8, or row 1 not fitting in part_len), -4 when the device
  * failed (CUDA error or a kernel wait that timed out; alto_last_error() has the reason).  Calls on one engine must
