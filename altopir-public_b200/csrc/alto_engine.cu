@@ -1009,7 +1009,7 @@ void *alto_engine_new(const uint8_t *db_col, const uint8_t *db_tiled, size_t ld,
   }
   if ((err = cudaStreamCreateWithFlags(&e->st_copy, cudaStreamNonBlocking)) != cudaSuccess) return fail("stream", err);
   if ((err = cudaEventCreate(&e->ev_begin)) != cudaSuccess || (err = cudaEventCreate(&e->ev_end)) != cudaSuccess ||
-      (err = cudaEventCreateWithFlags(&e->ev_keys, cudaEventDisableTiming)) != cudaSuccess ||
+      (err = cudaEventCreate(&e->ev_keys)) != cudaSuccess ||
       (err = cudaEventCreateWithFlags(&e->ev_queries, cudaEventDisableTiming)) != cudaSuccess ||
       (err = cudaEventCreate(&e->ev_pack)) != cudaSuccess || (err = cudaEventCreate(&e->ev_status)) != cudaSuccess)
     return fail("event", err);
