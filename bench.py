@@ -156,6 +156,25 @@ def traffic_from_profile(kernel, rows, record_bytes, batch):
         return None
 
 
+# ------------------------------------------------------------------------------------------------ ranks
+def max_over_ranks(x, world, device="cuda"):
+    """The largest value of x over all ranks (every rank gets it); the timing of a multi-GPU run is the slowest
+    rank's."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_qps(world, batch, steps, max_ms):
+    """Whole-job throughput: every rank answers `steps` batches of `batch` queries; the job takes the slowest
+    rank's time."""
+    return world * batch * steps / (max_ms * 1e-3)
+
+
 # ------------------------------------------------------------------------------------------------ reference arm
 def reference_state(a, svc):
     p = svc.params(a.rows, a.record_bytes)
@@ -317,13 +336,6 @@ def main_ours(a):
         if world > 1:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     # ---- warm-up (both paths)
     for _ in range(max(3, a.warmup)):
         e.enqueue_device(slots.data_ptr(), stride, B, d_out.data_ptr(), rl, d_status.data_ptr())
@@ -347,7 +359,7 @@ def main_ours(a):
     torch.cuda.synchronize()
     t1 = time.time()
     sampler.mark(t0, t1)
-    value_ms = max_over_ranks(s_ev.elapsed_time(e_ev))
+    value_ms = max_over_ranks(s_ev.elapsed_time(e_ev), world)
     kms, nb = e.kernel_times(reset=True)
     launches = e.last_launches() * a.steps
     assert (d_status == 0).all().item()
@@ -367,7 +379,7 @@ def main_ours(a):
     torch.cuda.synchronize()
     t1 = time.time()
     sampler.mark(t0, t1)
-    e2e_ms = max_over_ranks(s2.elapsed_time(e2))
+    e2e_ms = max_over_ranks(s2.elapsed_time(e2), world)
     host_out = h_out.numpy().copy()
     e.kernel_times(reset=True)
 
@@ -382,7 +394,7 @@ def main_ours(a):
         one[1].record(stream)
         e.sync()
         lat.append(one[0].elapsed_time(one[1]))
-    plain_total = max_over_ranks(sum(lat))
+    plain_total = max_over_ranks(sum(lat), world)
     sampler.stop()
 
     byte_exact_paths = bool(np.array_equal(dev_out, host_out))
@@ -420,8 +432,8 @@ def main_ours(a):
             exact_vs_ref = bool(np.array_equal(ref_out, dev_out))
 
     if rank == 0:
-        value = world * B * a.steps / (value_ms * 1e-3)
-        e2e = world * B * a.steps / (e2e_ms * 1e-3)
+        value = job_qps(world, B, a.steps, value_ms)
+        e2e = job_qps(world, B, a.steps, e2e_ms)
         lat_sorted = sorted(lat)
         line = {
             "metric": METRIC, "value": value, "unit": "QPS", "n_gpus": world, "steps": a.steps,
