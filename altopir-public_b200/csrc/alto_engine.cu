@@ -127,6 +127,10 @@ struct Batch {
   int *h_status = nullptr;
   uint32_t *d_err = nullptr, *h_err = nullptr;
   bool timing = false;  // record per-kernel timing marks into the engine's ring (main batch only)
+  // Side stream of the overlapped schedule: the query limb split beside the pack, and the tail of each column group
+  // but the last beside the scan of the next group.  It forks from and joins back into `st` inside every batch.
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_qready = nullptr, ev_join = nullptr, ev_scan[8] = {};
   // CUDA graphs of the device-side launch sequence, one per batch size and buffer set (see enqueue_batch)
   struct GraphEntry {
     size_t slots, stride, resp_stride;
@@ -178,6 +182,9 @@ struct Engine {
   CUtensorMap map_db, map_ub;
   int last_launches = 0;
   bool use_graphs = false;  // replay captured launch sequences (alto_engine_set_graphs)
+  bool overlap = true;      // the two-stream schedule of a batch (ALTO_OVERLAP=0 runs it on one stream)
+  int groups = 2;           // column groups of the scan and tail of a device batch (ALTO_GROUPS: 1, 2, 4 or 8)
+  int host_groups = 4;      // the same for alto_answer, whose groups' downloads overlap (ALTO_HOST_GROUPS)
   std::vector<TuneEntry> tuning;  // sorted by b_max; the first entry with b_max >= batch size applies
 };
 
@@ -276,7 +283,16 @@ void free_scratch(Batch *b) {
 
 // Stream, error word and its pinned mirror of a batch (scratch comes later, on demand).
 bool init_batch(Batch *b, bool timing) {
-  ALTO_CK(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
+  // The batch's stream has the highest priority and the side stream the lowest, so that when a GEMM and a tail are
+  // both waiting for SMs the GEMM's persistent CTAs are placed first and the tail's CTAs take the room left beside
+  // them, instead of the tail filling the SMs and holding the GEMM back.
+  int least = 0, greatest = 0;
+  ALTO_CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  ALTO_CK(cudaStreamCreateWithPriority(&b->st, cudaStreamNonBlocking, greatest));
+  ALTO_CK(cudaStreamCreateWithPriority(&b->side, cudaStreamNonBlocking, least));
+  for (cudaEvent_t *ev : {&b->ev_fork, &b->ev_qready, &b->ev_join})
+    ALTO_CK(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+  for (cudaEvent_t &ev : b->ev_scan) ALTO_CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   ALTO_CK(cudaMalloc(&b->d_err, sizeof(uint32_t)));
   ALTO_CK(cudaMemset(b->d_err, 0, sizeof(uint32_t)));
   ALTO_CK(cudaHostAlloc(&b->h_err, sizeof(uint32_t), cudaHostAllocDefault));
@@ -286,11 +302,17 @@ bool init_batch(Batch *b, bool timing) {
 
 void destroy_batch(Batch *b) {
   if (b->st) cudaStreamSynchronize(b->st);
+  if (b->side) cudaStreamSynchronize(b->side);
   free_scratch(b);
   cudaFree(b->d_err);
   cudaFreeHost(b->h_err);
+  for (cudaEvent_t ev : {b->ev_fork, b->ev_qready, b->ev_join})
+    if (ev) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : b->ev_scan)
+    if (ev) cudaEventDestroy(ev);
+  if (b->side) cudaStreamDestroy(b->side);
   if (b->st) cudaStreamDestroy(b->st);
-  b->st = nullptr;
+  b->st = b->side = nullptr;
   b->d_err = b->h_err = nullptr;
 }
 
@@ -319,6 +341,7 @@ void destroy(Engine *e) {
 bool ensure_capacity(const Engine *e, Batch *b, size_t slots) {
   if (slots <= b->cap) return true;
   ALTO_CK(cudaStreamSynchronize(b->st));
+  ALTO_CK(cudaStreamSynchronize(b->side));
   free_scratch(b);
   const size_t cap = round_up(slots, 4);
   ALTO_CK(cudaMalloc(&b->d_req, cap * e->slot_stride));
@@ -435,6 +458,8 @@ bool pair_kernels_enabled() {
   return !(v && strcmp(v, "single") == 0);
 }
 
+// The record-axis split is chosen for the whole scan; a scan run in column groups launches each group's share of
+// its units (splitting every group for its own tiles measured slower: more units, more partial-sum reductions).
 Plan make_plan(const Engine *e, size_t slots) {
   Plan p;
   const size_t limb_cols = 4 * round_up(slots, 4);
@@ -580,20 +605,97 @@ bool make_limb_maps(const Engine *e, const Plan &p, const uint8_t *qlimb, const 
          make_map(map_y, ylimb, e->count, 4 * (uint64_t)bp, e->count, box);
 }
 
-// Enqueues the answer path for `slots` staged frames on the engine's stream: validate, key limb split, pack GEMM,
-// then (after `queries_ready`, when the query words are still being uploaded on another stream) query limb split,
-// scan GEMM and tail.  The pack needs only the keys, so it overlaps the upload of the much larger query words.
-// Statuses go to d_status (and to the pinned host copy when host_status); responses of valid frames to
-// resp + slot * resp_stride.
+// Column groups of the scan and tail: whole response parts per group, an integral number of scan tiles each (`want`
+// lowered until both divide).
+int column_groups(const Engine *e, const Plan &p, int want) {
+  for (int g = want; g > 1; g /= 2)
+    if (e->outputs % g == 0 && p.scan_m % g == 0) return g;
+  return 1;
+}
+
+// Tail arguments for the output parts [o_begin, o_begin + o_count) of every frame.
+alto::TailArgs tail_args(const Engine *e, const Batch *bt, const uint8_t *d_slots, size_t slot_stride, uint8_t *resp,
+                         size_t resp_stride, int o_begin, int o_count) {
+  alto::TailArgs t;
+  t.acc = bt->d_acc;
+  t.beta = bt->d_beta;
+  t.status = bt->d_status;
+  t.req = d_slots;
+  t.req_stride = slot_stride;
+  t.z_off = kSlotLead + 9 + 4 * e->count;
+  t.that = e->d_that;
+  t.twiddle = e->d_tw;
+  t.prefix = e->d_prefix;
+  t.resp = resp;
+  t.resp_stride = resp_stride;
+  t.n = (int)e->n;
+  t.tg = (int)e->tg;
+  t.outputs = (int)e->outputs;
+  t.cols = (int)e->cols;
+  t.part_len = (int)e->part_len;
+  t.row1_off = (int)e->row1_off;
+  t.q1_bits = e->q1_bits;
+  t.q1 = (int64_t)e->q1;
+  t.o_begin = o_begin;
+  t.o_count = o_count;
+  return t;
+}
+
+// Query limb split and zeroing of the scan sums for `slots` staged frames, on stream st.
+bool enqueue_query_split(const Engine *e, const Batch *bt, const uint8_t *d_slots, size_t slot_stride, size_t slots,
+                         cudaStream_t st) {
+  const size_t bp = round_up(slots, 4), work = (e->rows / 16) * bp;
+  alto::limb_split_kernel<<<(unsigned)((work + 255) / 256), 256, 0, st>>>(
+      d_slots, slot_stride, kSlotLead + 9 + 8 * e->count, (int)slots, (int)bp, e->rows, e->chunk, bt->d_qlimb);
+  ALTO_CK(cudaGetLastError());
+  ALTO_CK(cudaMemsetAsync(bt->d_acc, 0, slots * e->cols * sizeof(uint32_t), st));
+  return true;
+}
+
+// Scan and tail in column groups.  With the overlapped schedule the tail of every group but the last runs on the
+// side stream beside the scan of the next group (the tail is integer-ALU work, the scan tensor work, and an SM has
+// room for a tail CTA next to a GEMM CTA); `done[g]`, when given, is recorded after the tail of group g.
+bool enqueue_scan_tails(Engine *e, Batch *bt, const Plan &p, const CUtensorMap &map_q, const uint8_t *d_slots,
+                        size_t slot_stride, size_t slots, uint8_t *resp, size_t resp_stride, int groups,
+                        const cudaEvent_t *done, int *launches, cudaEvent_t before_last_tail = nullptr) {
+  cudaStream_t st = bt->st;
+  const int parts = (int)e->outputs / groups;
+  for (int g = 0; g < groups; ++g) {
+    if (!launch_scan(e, p, map_q, bt->d_acc, slots, st, bt->d_err, g, groups)) return false;
+    const bool last = g + 1 == groups;
+    cudaStream_t ts = last ? st : bt->side;
+    if (!last) {
+      ALTO_CK(cudaEventRecord(bt->ev_scan[g], st));
+      ALTO_CK(cudaStreamWaitEvent(ts, bt->ev_scan[g], 0));
+    } else if (before_last_tail) {
+      ALTO_CK(cudaEventRecord(before_last_tail, st));
+    }
+    ALTO_CK(alto::launch_tail(tail_args(e, bt, d_slots, slot_stride, resp, resp_stride, g * parts, parts), slots, ts));
+    *launches += 2;
+    if (done) ALTO_CK(cudaEventRecord(done[g], ts));
+  }
+  if (groups > 1) {  // join the side stream's tails
+    ALTO_CK(cudaEventRecord(bt->ev_join, bt->side));
+    ALTO_CK(cudaStreamWaitEvent(st, bt->ev_join, 0));
+  }
+  return true;
+}
+
+// Enqueues the answer path for `slots` staged frames on the batch's stream: validate, key limb split, pack GEMM,
+// query limb split, scan GEMM and tail.  Statuses go to d_status (and to the pinned host copy when host_status);
+// responses of valid frames to resp + slot * resp_stride.  With the overlapped schedule the query limb split and the
+// zeroing of the scan sums run on the side stream beside validation and the pack, and the tails of all column groups
+// but the last beside the scan (enqueue_scan_tails); the side stream forks from and joins back into the batch's
+// stream, so the batch is complete when its stream passes it.
 bool enqueue_batch_direct(Engine *e, Batch *bt, const uint8_t *d_slots, size_t slot_stride, size_t slots,
-                          uint8_t *resp, size_t resp_stride, bool host_status, cudaEvent_t queries_ready,
-                          bool with_marks) {
+                          uint8_t *resp, size_t resp_stride, bool host_status, bool with_marks) {
   cudaStream_t st = bt->st;
   const Plan p = make_plan(e, slots);
+  const int groups = e->overlap ? column_groups(e, p, e->groups) : 1;
   const int bp = (int)round_up(slots, 4);
   int launches = 0;
-  // timing marks (main batch only): 0 begin | validate | 1 | y split | 2 | pack | 3 | (query wait) q split,
-  // zeroing | 4 | scan | 5 | tail | 6
+  // timing marks (main batch only): 0 begin | validate | 1 | y split | 2 | pack | 3 | (wait for the query split)
+  // | 4 | scan (with all tails but the last beside it) | 5 | last tail | 6
   cudaEvent_t *mk = nullptr;
   if (bt->timing && with_marks) {
     int set = 0;
@@ -602,6 +704,13 @@ bool enqueue_batch_direct(Engine *e, Batch *bt, const uint8_t *d_slots, size_t s
   }
   auto mark = [&](int i) { return mk ? cudaEventRecord(mk[i], st) : cudaSuccess; };
   ALTO_CK(mark(0));
+  if (e->overlap) {
+    ALTO_CK(cudaEventRecord(bt->ev_fork, st));
+    ALTO_CK(cudaStreamWaitEvent(bt->side, bt->ev_fork, 0));
+    if (!enqueue_query_split(e, bt, d_slots, slot_stride, slots, bt->side)) return false;
+    launches += 1;
+    ALTO_CK(cudaEventRecord(bt->ev_qready, bt->side));
+  }
 
   alto::validate_kernel<<<(unsigned)slots, 256, 0, st>>>(d_slots, slot_stride, kSlotLead, e->count, e->rows,
                                                          bt->d_status);
@@ -612,10 +721,9 @@ bool enqueue_batch_direct(Engine *e, Batch *bt, const uint8_t *d_slots, size_t s
 
   CUtensorMap map_q, map_y;
   if (!make_limb_maps(e, p, bt->d_qlimb, bt->d_ylimb, bp, &map_q, &map_y)) return false;
-  const unsigned split_threads = 256;
   {
     const size_t work = (e->count / 16) * (size_t)bp;
-    alto::limb_split_kernel<<<(unsigned)((work + split_threads - 1) / split_threads), split_threads, 0, st>>>(
+    alto::limb_split_kernel<<<(unsigned)((work + 255) / 256), 256, 0, st>>>(
         d_slots, slot_stride, kSlotLead + 9, (int)slots, bp, e->count, e->count, bt->d_ylimb);
     ++launches;
     ALTO_CK(cudaGetLastError());
@@ -624,58 +732,28 @@ bool enqueue_batch_direct(Engine *e, Batch *bt, const uint8_t *d_slots, size_t s
   if (!launch_pack(e, p, map_y, bt->d_beta, slots, st, bt->d_err)) return false;
   ++launches;
   ALTO_CK(mark(3));
-  if (queries_ready) ALTO_CK(cudaStreamWaitEvent(st, queries_ready, 0));
-  {
-    const size_t work = (e->rows / 16) * (size_t)bp;
-    alto::limb_split_kernel<<<(unsigned)((work + split_threads - 1) / split_threads), split_threads, 0, st>>>(
-        d_slots, slot_stride, kSlotLead + 9 + 8 * e->count, (int)slots, bp, e->rows, e->chunk, bt->d_qlimb);
-    ++launches;
-    ALTO_CK(cudaGetLastError());
+  if (e->overlap) {
+    ALTO_CK(cudaStreamWaitEvent(st, bt->ev_qready, 0));
+  } else {
+    if (!enqueue_query_split(e, bt, d_slots, slot_stride, slots, st)) return false;
+    launches += 1;
   }
-  ALTO_CK(cudaMemsetAsync(bt->d_acc, 0, slots * e->cols * sizeof(uint32_t), st));
   ALTO_CK(mark(4));
-  if (!launch_scan(e, p, map_q, bt->d_acc, slots, st, bt->d_err)) return false;
-  ++launches;
-  ALTO_CK(mark(5));
-  {
-    alto::TailArgs t;
-    t.acc = bt->d_acc;
-    t.beta = bt->d_beta;
-    t.status = bt->d_status;
-    t.req = d_slots;
-    t.req_stride = slot_stride;
-    t.z_off = kSlotLead + 9 + 4 * e->count;
-    t.that = e->d_that;
-    t.twiddle = e->d_tw;
-    t.prefix = e->d_prefix;
-    t.resp = resp;
-    t.resp_stride = resp_stride;
-    t.n = (int)e->n;
-    t.tg = (int)e->tg;
-    t.outputs = (int)e->outputs;
-    t.cols = (int)e->cols;
-    t.part_len = (int)e->part_len;
-    t.row1_off = (int)e->row1_off;
-    t.q1_bits = e->q1_bits;
-    t.q1 = (int64_t)e->q1;
-    t.o_begin = 0;
-    t.o_count = (int)e->outputs;
-    ALTO_CK(alto::launch_tail(t, slots, st));
-    ++launches;
-  }
+  if (!enqueue_scan_tails(e, bt, p, map_q, d_slots, slot_stride, slots, resp, resp_stride, groups, nullptr, &launches,
+                          mk ? mk[5] : nullptr))
+    return false;
   ALTO_CK(mark(6));
   e->last_launches = launches;
   return true;
 }
 
-// enqueue_batch_direct, or -- when the engine replays graphs and the batch does not wait on another stream -- the
-// same sequence as a CUDA graph captured on first use for this batch size and these buffers and replayed after.
+// enqueue_batch_direct, or -- when the engine replays graphs -- the same sequence (both streams) as a CUDA graph
+// captured on first use for this batch size and these buffers and replayed after.
 // Graph replays record no per-kernel timing marks.
 bool enqueue_batch(Engine *e, Batch *bt, const uint8_t *d_slots, size_t slot_stride, size_t slots, uint8_t *resp,
-                   size_t resp_stride, bool host_status, cudaEvent_t queries_ready = nullptr) {
-  if (!e->use_graphs || queries_ready)
-    return enqueue_batch_direct(e, bt, d_slots, slot_stride, slots, resp, resp_stride, host_status, queries_ready,
-                                true);
+                   size_t resp_stride, bool host_status) {
+  if (!e->use_graphs)
+    return enqueue_batch_direct(e, bt, d_slots, slot_stride, slots, resp, resp_stride, host_status, true);
   for (const Batch::GraphEntry &g : bt->graphs)
     if (g.slots == slots && g.d_slots == d_slots && g.stride == slot_stride && g.resp == resp &&
         g.resp_stride == resp_stride && g.host_status == host_status) {
@@ -684,7 +762,7 @@ bool enqueue_batch(Engine *e, Batch *bt, const uint8_t *d_slots, size_t slot_str
     }
   ALTO_CK(cudaStreamBeginCapture(bt->st, cudaStreamCaptureModeThreadLocal));
   const bool ok =
-      enqueue_batch_direct(e, bt, d_slots, slot_stride, slots, resp, resp_stride, host_status, nullptr, false);
+      enqueue_batch_direct(e, bt, d_slots, slot_stride, slots, resp, resp_stride, host_status, false);
   cudaGraph_t graph = nullptr;
   const cudaError_t end = cudaStreamEndCapture(bt->st, &graph);
   if (!ok || end != cudaSuccess) {
@@ -784,19 +862,10 @@ bool host_header_status(const Engine *e, const uint8_t *f, size_t len, int *stat
   return true;
 }
 
-// Column groups of the host pipeline: whole response parts per group, an integral number of scan tiles each.
-// ALTO_HOST_GROUPS (1, 2, 4 or 8) overrides the default of two.
-int host_groups(const Engine *e, const Plan &p) {
-  int want = 2;
-  if (const char *v = getenv("ALTO_HOST_GROUPS")) want = std::max(1, std::min(8, atoi(v)));
-  for (int g = want; g > 1; g /= 2)
-    if (e->outputs % g == 0 && p.scan_m % g == 0) return g;
-  return 1;
-}
-
 // alto_answer: header and y keys upload first and the pack starts on them while z keys and query words upload on
 // the copy stream; then validation, the query limb split, and the scan and tail in column groups.  The responses of
-// a group download (valid frames only, on the copy stream) while the next group computes.
+// a group download (valid frames only, on the copy stream) while the next group computes.  Without the overlapped
+// schedule (ALTO_OVERLAP=0) everything but the uploads and downloads runs on the batch's stream, in one group.
 int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t b, uint8_t *const *out, int *status,
                 double *stage_ms) {
   std::vector<size_t> cand;
@@ -824,7 +893,7 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
   cudaStream_t st = bt->st, sc = e->st_copy;
   const size_t nc = cand.size();
   const Plan p = make_plan(e, nc);
-  const int groups = host_groups(e, p);
+  const int groups = e->overlap ? column_groups(e, p, e->host_groups) : 1;
   const int bp = (int)round_up(nc, 4);
   const size_t ybytes = 9 + 4 * e->count;  // header and y keys
   int launches = 0;
@@ -852,10 +921,9 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
 
   CUtensorMap map_q, map_y;
   if (!make_limb_maps(e, p, bt->d_qlimb, bt->d_ylimb, bp, &map_q, &map_y)) return -4;
-  const unsigned tpb = 256;
   {
     const size_t work = (e->count / 16) * (size_t)bp;
-    alto::limb_split_kernel<<<(unsigned)((work + tpb - 1) / tpb), tpb, 0, st>>>(
+    alto::limb_split_kernel<<<(unsigned)((work + 255) / 256), 256, 0, st>>>(
         bt->d_req, e->slot_stride, kSlotLead + 9, (int)nc, bp, e->count, e->count, bt->d_ylimb);
     ALTO_H(cudaGetLastError());
     ++launches;
@@ -863,50 +931,25 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
   if (!launch_pack(e, p, map_y, bt->d_beta, nc, st, bt->d_err)) return -4;
   ++launches;
   ALTO_H(cudaEventRecord(e->ev_pack, st));
-  ALTO_H(cudaStreamWaitEvent(st, e->ev_queries, 0));
-  alto::validate_kernel<<<(unsigned)nc, 256, 0, st>>>(bt->d_req, e->slot_stride, kSlotLead, e->count, e->rows,
+  // validation, the status download, the query limb split and the zeroing of the scan sums: on the side stream
+  // beside the pack once the query words are in (on the batch's stream after the pack without the overlap)
+  cudaStream_t vs = e->overlap ? bt->side : st;
+  ALTO_H(cudaStreamWaitEvent(vs, e->ev_queries, 0));
+  alto::validate_kernel<<<(unsigned)nc, 256, 0, vs>>>(bt->d_req, e->slot_stride, kSlotLead, e->count, e->rows,
                                                       bt->d_status);
   ALTO_H(cudaGetLastError());
   ++launches;
-  ALTO_H(cudaMemcpyAsync(bt->h_status, bt->d_status, nc * sizeof(int), cudaMemcpyDeviceToHost, st));
-  ALTO_H(cudaEventRecord(e->ev_status, st));
-  {
-    const size_t work = (e->rows / 16) * (size_t)bp;
-    alto::limb_split_kernel<<<(unsigned)((work + tpb - 1) / tpb), tpb, 0, st>>>(
-        bt->d_req, e->slot_stride, kSlotLead + 9 + 8 * e->count, (int)nc, bp, e->rows, e->chunk, bt->d_qlimb);
-    ALTO_H(cudaGetLastError());
-    ++launches;
+  ALTO_H(cudaMemcpyAsync(bt->h_status, bt->d_status, nc * sizeof(int), cudaMemcpyDeviceToHost, vs));
+  ALTO_H(cudaEventRecord(e->ev_status, vs));
+  if (!enqueue_query_split(e, bt, bt->d_req, e->slot_stride, nc, vs)) return -4;
+  ++launches;
+  if (e->overlap) {
+    ALTO_H(cudaEventRecord(bt->ev_qready, vs));
+    ALTO_H(cudaStreamWaitEvent(st, bt->ev_qready, 0));
   }
-  ALTO_H(cudaMemsetAsync(bt->d_acc, 0, nc * e->cols * sizeof(uint32_t), st));
-  const int parts = (int)e->outputs / groups;
-  for (int g = 0; g < groups; ++g) {
-    if (!launch_scan(e, p, map_q, bt->d_acc, nc, st, bt->d_err, g, groups)) return -4;
-    alto::TailArgs t;
-    t.acc = bt->d_acc;
-    t.beta = bt->d_beta;
-    t.status = bt->d_status;
-    t.req = bt->d_req;
-    t.req_stride = e->slot_stride;
-    t.z_off = kSlotLead + 9 + 4 * e->count;
-    t.that = e->d_that;
-    t.twiddle = e->d_tw;
-    t.prefix = e->d_prefix;
-    t.resp = bt->d_resp;
-    t.resp_stride = e->resp_len;
-    t.n = (int)e->n;
-    t.tg = (int)e->tg;
-    t.outputs = (int)e->outputs;
-    t.cols = (int)e->cols;
-    t.part_len = (int)e->part_len;
-    t.row1_off = (int)e->row1_off;
-    t.q1_bits = e->q1_bits;
-    t.q1 = (int64_t)e->q1;
-    t.o_begin = g * parts;
-    t.o_count = parts;
-    ALTO_H(alto::launch_tail(t, nc, st));
-    launches += 2;
-    ALTO_H(cudaEventRecord(e->ev_group[g], st));
-  }
+  if (!enqueue_scan_tails(e, bt, p, map_q, bt->d_req, e->slot_stride, nc, bt->d_resp, e->resp_len, groups,
+                          e->ev_group, &launches))
+    return -4;
   e->last_launches = launches;
 
   // statuses come back as soon as validation is done; then each group's valid responses download on the copy
@@ -917,7 +960,7 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
     status[cand[i]] = bt->h_status[i];
     if (bt->h_status[i] == 0) ok.push_back(i);
   }
-  const size_t gbytes = (size_t)parts * e->part_len;
+  const size_t gbytes = (size_t)(e->outputs / groups) * e->part_len;
   for (int g = 0; g < groups; ++g) {
     ALTO_H(cudaStreamWaitEvent(sc, e->ev_group[g], 0));
     const size_t off = (size_t)g * gbytes;
@@ -1008,6 +1051,9 @@ void *alto_engine_new(const uint8_t *db_col, const uint8_t *db_tiled, size_t ld,
     return nullptr;
   }
   if ((err = cudaStreamCreateWithFlags(&e->st_copy, cudaStreamNonBlocking)) != cudaSuccess) return fail("stream", err);
+  if (const char *v = getenv("ALTO_OVERLAP")) e->overlap = v[0] != '0';
+  if (const char *v = getenv("ALTO_GROUPS")) e->groups = std::max(1, std::min(8, atoi(v)));
+  if (const char *v = getenv("ALTO_HOST_GROUPS")) e->host_groups = std::max(1, std::min(8, atoi(v)));
   if ((err = cudaEventCreate(&e->ev_begin)) != cudaSuccess || (err = cudaEventCreate(&e->ev_end)) != cudaSuccess ||
       (err = cudaEventCreate(&e->ev_keys)) != cudaSuccess ||
       (err = cudaEventCreateWithFlags(&e->ev_queries, cudaEventDisableTiming)) != cudaSuccess ||

@@ -202,3 +202,35 @@ def test_every_plan_and_the_graph_path_return_identical_bytes(gpu, svc, eng):
         assert np.array_equal(out.cpu().numpy(), want[:bb]), bb
     e.set_graphs(False)
     e.close()
+
+
+def test_every_schedule_returns_identical_bytes(gpu, svc, eng, monkeypatch):
+    # one stream or two (ALTO_OVERLAP), and 1..8 column groups for the device path (ALTO_GROUPS) and alto_answer
+    # (ALTO_HOST_GROUPS); the knobs are read when an engine is created
+    import torch
+    p = svc.params(4096, 32768)  # 16 response parts, so every group count divides
+    st = svc.SyntheticState.make(p, seed=41)
+    b = 24
+    frames = svc.synthetic_requests(p, b, seed=42)
+    frames[3, 9:13] = 0xFF  # y[0] >= Q: status 3
+    want = None
+    for overlap, groups, host_groups in ((0, 1, 1), (1, 1, 1), (1, 2, 2), (1, 4, 4), (1, 8, 8), (1, 2, 4)):
+        monkeypatch.setenv("ALTO_OVERLAP", str(overlap))
+        monkeypatch.setenv("ALTO_GROUPS", str(groups))
+        monkeypatch.setenv("ALTO_HOST_GROUPS", str(host_groups))
+        e = eng.Engine.from_state(st)
+        ql, rl = e.request_len(), e.response_len()
+        n, status, host = _answer(e, [frames[i] for i in range(b)], fill=0x11)
+        stride = (7 + ql + 15) // 16 * 16
+        slots = torch.zeros((b, stride), dtype=torch.uint8, device="cuda")
+        slots[:, 7:7 + ql] = torch.from_numpy(frames).cuda()
+        out = torch.full((b, rl), 0x11, dtype=torch.uint8, device="cuda")
+        dstat = np.full(b, -1, dtype=np.int32)
+        assert e.answer_device(slots.data_ptr(), stride, b, out.data_ptr(), rl, dstat) == b - 1
+        assert n == b - 1 and status[3] == 3 and list(dstat) == list(status)
+        dev = out.cpu().numpy()
+        assert np.array_equal(dev, host) and (host[3] == 0x11).all()
+        if want is None:
+            want = host
+        assert np.array_equal(host, want), (overlap, groups, host_groups)
+        e.close()
