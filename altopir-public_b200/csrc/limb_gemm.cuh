@@ -1,12 +1,14 @@
 // limb_gemm.cuh -- the two dense contractions of the answer path as tcgen05 kind::i8 GEMMs over byte limbs.
 //
 //   scan (src/amx_kernels.cpp:175-309): A = database, one row per record byte position (column of the record
-//        matrix), K = records, K-major in HBM exactly as the server's column-order database; B = the batch's query
+//        matrix), K = records, K-major (the server's column-order database) and stored tile by tile: every
+//        128-row x 128-byte tile is 16 KB contiguous in HBM (see the engine's set-up); B = the batch's query
 //        words split into 4 byte limbs, one row per (client, limb).  D[col][(c, j)] = sum_k db[col][k] * q_c[k]_j.
 //        Epilogue: acc = sum_j D << 8j (mod 2^32), added into acc[c][col] with a 32-bit reduction so that split-K
 //        chunks (each short enough that no int32 partial sum can overflow) combine modulo 2^32.
 //   pack (src/amx_kernels.cpp:345-445): A = the packing matrix as 4 byte planes, rows ordered (col, plane j),
-//        K = tg * n; B = the packing keys y split into 4 byte limbs, rows (client, limb i).
+//        K = tg * n, stored tile by tile like the database; B = the packing keys y split into 4 byte limbs, rows
+//        (client, limb i).
 //        Epilogue: beta[c][col] = sum_{i,j} D[(col, j)][(c, i)] * 2^(8(i+j)) mod Q, the 4 planes of one column
 //        sitting in 4 adjacent TMEM lanes of one warp and combined with two shuffles.
 //
@@ -36,7 +38,7 @@ struct GemmArgs {
   uint32_t *out;    // scan: acc[c * cols + col], pre-zeroed; pack: beta[c * cols + col]
   uint32_t *err;    // device error word
   int b_keep;       // 1: keep the B operand in L2 (evict_last; it is small and read by every unit), 0: normal
-  int kb_chunk;     // scan: 128-byte blocks per record chunk of the 3-D operand maps (units never straddle chunks)
+  int kb_chunk;     // scan: 128-byte blocks per record chunk of the 3-D query-limb map (units never straddle chunks)
   int m_begin;      // first tile along A (a launch may cover a column group: tiles m_begin .. m_begin + num_m)
 };
 
@@ -125,10 +127,10 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         if constexpr (EPI == Epi::kScan) {
           // record chunk z, 128-byte block x inside it
           const int kb = kb0 + i, z = kb / args.kb_chunk, x = (kb - z * args.kb_chunk) * kBK;
-          tma_load_3d(sa, &map_a, full0 + 8 * s, x, m_tile * kBM, z, pol_a);
+          tma_load_tile(sa, &map_a, full0 + 8 * s, kb, m_tile, pol_a);
           tma_load_3d(sb, &map_b, full0 + 8 * s, x, n_tile * BN, z, pol_b);
         } else {
-          tma_load_2d(sa, &map_a, full0 + 8 * s, (kb0 + i) * kBK, m_tile * kBM, pol_a);
+          tma_load_tile(sa, &map_a, full0 + 8 * s, kb0 + i, m_tile, pol_a);
           tma_load_2d(sb, &map_b, full0 + 8 * s, (kb0 + i) * kBK, n_tile * BN, pol_b);
         }
         issued = i + 1;

@@ -52,7 +52,7 @@ struct PairArgs {
   uint32_t *out;    // scan: acc[c * cols + col] (pre-zeroed, summed mod 2^32); pack: beta[c * cols + col]
   uint32_t *err;    // device error word
   int b_keep;       // 1: keep the B operand in L2 (evict_last; it is small and read by every unit), 0: normal
-  int kb_chunk;     // scan: 128-byte blocks per record chunk of the 3-D operand maps (units never straddle chunks)
+  int kb_chunk;     // scan: 128-byte blocks per record chunk of the 3-D query-limb map (units never straddle chunks)
   int m_begin;      // first 256-row tile along A (a launch may cover a column group)
 };
 
@@ -166,14 +166,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
           if (leader) mbar_arrive_expect_tx(full0 + 8 * s, 2 * S::kStageBytes);
           if constexpr (EPI == Epi::kScan) {
             const int kb = kb0 + i, z = kb / args.kb_chunk, x = (kb - z * args.kb_chunk) * kBK;
-            tma_load_3d_pair(sa, &map_a, full_leader0 + 8 * s, x, m * 256 + (int)rank * 128, z, pol_a);
+            tma_load_tile_pair(sa, &map_a, full_leader0 + 8 * s, kb, 2 * m + (int)rank, pol_a);
 #pragma unroll
             for (int t = 0; t < NSUB; ++t)
               tma_load_3d_pair(sb + t * (BN / 2) * kBK, &map_b, full_leader0 + 8 * s, x,
                                (n * NSUB + t) * BN + (int)rank * (BN / 2), z, pol_b);
           } else {
             const int x = (kb0 + i) * kBK;
-            tma_load_2d_pair(sa, &map_a, full_leader0 + 8 * s, x, m * 256 + (int)rank * 128, pol_a);
+            tma_load_tile_pair(sa, &map_a, full_leader0 + 8 * s, kb0 + i, 2 * m + (int)rank, pol_a);
 #pragma unroll
             for (int t = 0; t < NSUB; ++t)
               tma_load_2d_pair(sb + t * (BN / 2) * kBK, &map_b, full_leader0 + 8 * s, x,

@@ -93,6 +93,16 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
       "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y), "r"(z), "l"(cache_hint)
       : "memory");
 }
+// 4-D tiled load of one tile of a tile-contiguous operand: coordinates (0, 0, k block, 128-row tile), the box being
+// the whole 128 x 128-byte tile (16 KB contiguous in global memory).
+__device__ __forceinline__ void tma_load_tile(uint32_t dst, const CUtensorMap *map, uint32_t bar, int32_t kb,
+                                              int32_t mt, uint64_t cache_hint) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+      " [%0], [%1, {%3, %3, %4, %5}], [%2], %6;" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(0), "r"(kb), "r"(mt), "l"(cache_hint)
+      : "memory");
+}
 // L2 cache policies for the loads (createpolicy fractions of 1.0).
 __device__ __forceinline__ uint64_t policy_evict_first() {
   uint64_t p;
@@ -212,6 +222,14 @@ __device__ __forceinline__ void tma_load_3d_pair(uint32_t dst, const CUtensorMap
       "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
       " [%0], [%1, {%3, %4, %5}], [%2], %6;" ::"r"(dst),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(bar_cluster), "r"(x), "r"(y), "r"(z), "l"(cache_hint)
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_tile_pair(uint32_t dst, const CUtensorMap *map, uint32_t bar_cluster,
+                                                   int32_t kb, int32_t mt, uint64_t cache_hint) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+      " [%0], [%1, {%3, %3, %4, %5}], [%2], %6;" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(bar_cluster), "r"(0), "r"(kb), "r"(mt), "l"(cache_hint)
       : "memory");
 }
 __device__ __forceinline__ void tmem_alloc_pair(uint32_t dst_smem, uint32_t ncols) {
