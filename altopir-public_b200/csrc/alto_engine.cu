@@ -137,26 +137,29 @@ bool make_tile_map(CUtensorMap *m, const void *base, uint64_t kbs, uint64_t mts)
 size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 // Uploads a row-major host matrix (nrows rows of k_bytes bytes, row pitch `pitch`) into the tile-contiguous layout
-// of kbs x mts tiles at dst (zero where rows or bytes run past the matrix), through a device staging buffer of 128
-// rows x at most 128 KB: one pass per 128-row tile and slab of columns.  Runs on the legacy default stream, which
-// orders each staging copy after the previous rearrangement.
+// of kbs x mts tiles at dst (zero where rows or bytes run past the matrix), through a 16 MB device staging buffer: one
+// pass per slab of at most 128 KB of every row and as many 128-row tiles as fit.  Runs on the legacy default stream,
+// which orders each staging copy after the previous rearrangement.
 bool upload_tiled(uint8_t *dst, const uint8_t *src, size_t pitch, size_t nrows, size_t k_bytes, size_t kbs,
                   size_t mts) {
+  const size_t stage_bytes = size_t(16) << 20;
   const size_t slab = std::min<size_t>(kbs * 128, 131072);
+  const size_t per_pass = std::max<size_t>(1, stage_bytes / (128 * slab));  // row tiles per pass
   uint8_t *stage = nullptr;
-  ALTO_CK(cudaMalloc(&stage, 128 * slab));
+  ALTO_CK(cudaMalloc(&stage, per_pass * 128 * slab));
   bool ok = true;
-  for (size_t mt = 0; mt < mts && ok; ++mt) {
-    const size_t r0 = mt * 128, nr = r0 < nrows ? std::min<size_t>(128, nrows - r0) : 0;
+  for (size_t mt = 0; mt < mts && ok; mt += per_pass) {
+    const size_t ntr = std::min(per_pass, mts - mt);
+    const size_t r0 = mt * 128, nr = r0 < nrows ? std::min(ntr * 128, nrows - r0) : 0;
     for (size_t k0 = 0; k0 < kbs * 128 && ok; k0 += slab) {
       const size_t nk = k0 < k_bytes ? std::min(slab, k_bytes - k0) : 0;
       const size_t tiles = std::min(slab, kbs * 128 - k0) / 128;
       cudaError_t err = cudaSuccess;
       if (nr && nk) err = cudaMemcpy2D(stage, slab, src + r0 * pitch + k0, pitch, nk, nr, cudaMemcpyHostToDevice);
       if (err == cudaSuccess) {
-        const size_t words = tiles * 1024;  // 16-byte words of output
-        alto::tile_slab_kernel<<<(unsigned)((words + 255) / 256), 256>>>(stage, slab, (int)nr, (int)nk, words,
-                                                                         dst + (mt * kbs + k0 / 128) * 16384);
+        const size_t words = ntr * tiles * 1024;  // 16-byte words of output
+        alto::tile_slab_kernel<<<(unsigned)((words + 255) / 256), 256>>>(
+            stage, slab, (int)nr, (int)nk, (int)tiles, words, dst + mt * kbs * 16384, kbs, k0 / 128);
         err = cudaGetLastError();
       }
       if (err != cudaSuccess) {
@@ -250,7 +253,8 @@ struct Engine {
   bool use_graphs = false;  // replay captured launch sequences (alto_engine_set_graphs)
   bool overlap = true;      // the two-stream schedule of a batch (ALTO_OVERLAP=0 runs it on one stream)
   int groups = 2;           // column groups of the scan and tail of a device batch (ALTO_GROUPS: 1, 2, 4 or 8)
-  int host_groups = 4;      // the same for alto_answer, whose groups' downloads overlap (ALTO_HOST_GROUPS)
+  int host_groups = 4;      // the same for alto_answer, whose groups' downloads overlap (ALTO_HOST_GROUPS); its
+                            // last group is half the size of the others (less left to download after the last scan)
   std::vector<TuneEntry> tuning;  // sorted by b_max; the first entry with b_max >= batch size applies
 };
 
@@ -586,9 +590,9 @@ Plan make_plan(const Engine *e, size_t slots) {
 
 // The scan GEMM (acc sums, pre-zeroed) and the pack GEMM (beta) for `slots` clients under plan p.
 bool launch_scan(const Engine *e, const Plan &p, const CUtensorMap &map_q, uint32_t *acc, size_t slots,
-                 cudaStream_t st, uint32_t *err, int group = 0, int groups = 1) {
-  // column group `group` of `groups`: scan tiles [m0, m0 + mg) (the plan's tile count divides by the groups)
-  const int mg = p.scan_m / groups, m0 = group * mg;
+                 cudaStream_t st, uint32_t *err, int m0 = 0, int mg = -1) {
+  // scan tiles [m0, m0 + mg) along the database columns (all of them by default)
+  if (mg < 0) mg = p.scan_m;
   // The query limbs are re-read by every unit of a K chunk; mark them evict-last only while the whole operand
   // (4 bytes per record and client) is a small part of the 126 MB L2, so stale chunks never crowd it out.
   const int keep_b = 4 * round_up(slots, 4) * e->rows <= (size_t(32) << 20);
@@ -671,12 +675,37 @@ bool make_limb_maps(const Engine *e, const Plan &p, const uint8_t *qlimb, const 
          make_map(map_y, ylimb, e->count, 4 * (uint64_t)bp, e->count, box);
 }
 
-// Column groups of the scan and tail: whole response parts per group, an integral number of scan tiles each (`want`
-// lowered until both divide).
-int column_groups(const Engine *e, const Plan &p, int want) {
-  for (int g = want; g > 1; g /= 2)
-    if (e->outputs % g == 0 && p.scan_m % g == 0) return g;
-  return 1;
+// Column groups of the scan and tail: group g is the response parts [bounds[g], bounds[g + 1]), whose columns are
+// whole scan tiles (a part is n columns; a tile 256 columns for the pair kernels, 128 for the single-CTA ones).
+struct Groups {
+  int count = 1;
+  int bounds[9] = {0};
+  int tiles_per_part = 0;
+};
+
+// `want` groups of (nearly) equal size, or with `small_last` a last group of half the size of the others, so that
+// less of the work -- its tail and, in alto_answer, its download -- is left once the last scan ends.
+Groups column_groups(const Engine *e, const Plan &p, int want, bool small_last = false) {
+  Groups g;
+  const int tile_cols = p.pair ? 256 : 128;
+  g.bounds[1] = (int)e->outputs;
+  if (want <= 1 || e->n % tile_cols) return g;
+  g.tiles_per_part = (int)(e->n / tile_cols);
+  const int count = std::min<int>(std::min(want, 8), (int)e->outputs);
+  // weights: 2 for every group, 1 for a small last one
+  const int total = 2 * count - (small_last ? 1 : 0);
+  int acc = 0;
+  for (int i = 0; i < count; ++i) {
+    acc += (small_last && i + 1 == count) ? 1 : 2;
+    g.bounds[i + 1] = (int)((e->outputs * (size_t)acc + total / 2) / total);
+  }
+  g.bounds[count] = (int)e->outputs;
+  // drop empty groups
+  int k = 0;
+  for (int i = 1; i <= count; ++i)
+    if (g.bounds[i] > g.bounds[k]) g.bounds[++k] = g.bounds[i];
+  g.count = k;
+  return g;
 }
 
 // Tail arguments for the output parts [o_begin, o_begin + o_count) of every frame.
@@ -718,29 +747,35 @@ bool enqueue_query_split(const Engine *e, const Batch *bt, const uint8_t *d_slot
   return true;
 }
 
-// Scan and tail in column groups.  With the overlapped schedule the tail of every group but the last runs on the
-// side stream beside the scan of the next group (the tail is integer-ALU work, the scan tensor work, and an SM has
-// room for a tail CTA next to a GEMM CTA); `done[g]`, when given, is recorded after the tail of group g.
+// Scan and tail in column groups: the tail of every group but the last runs on the side stream beside the scan of the
+// next group (the tail is integer-ALU work, the scan tensor work; the side stream's lower priority lets the scan's
+// CTAs be placed first); `done[g]`, when given, is recorded after the tail of group g.
 bool enqueue_scan_tails(Engine *e, Batch *bt, const Plan &p, const CUtensorMap &map_q, const uint8_t *d_slots,
-                        size_t slot_stride, size_t slots, uint8_t *resp, size_t resp_stride, int groups,
-                        const cudaEvent_t *done, int *launches, cudaEvent_t before_last_tail = nullptr) {
+                        size_t slot_stride, size_t slots, uint8_t *resp, size_t resp_stride, const Groups &gr,
+                        const cudaEvent_t *done, int *launches,
+                        cudaEvent_t before_last_tail = nullptr) {
   cudaStream_t st = bt->st;
-  const int parts = (int)e->outputs / groups;
-  for (int g = 0; g < groups; ++g) {
-    if (!launch_scan(e, p, map_q, bt->d_acc, slots, st, bt->d_err, g, groups)) return false;
-    const bool last = g + 1 == groups;
+  bool forked = false;
+  for (int g = 0; g < gr.count; ++g) {
+    const int o0 = gr.bounds[g], parts = gr.bounds[g + 1] - o0;
+    const bool ok = gr.count == 1 ? launch_scan(e, p, map_q, bt->d_acc, slots, st, bt->d_err)
+                                  : launch_scan(e, p, map_q, bt->d_acc, slots, st, bt->d_err, o0 * gr.tiles_per_part,
+                                                parts * gr.tiles_per_part);
+    if (!ok) return false;
+    const bool last = g + 1 == gr.count;
     cudaStream_t ts = last ? st : bt->side;
-    if (!last) {
+    if (ts != st) {
       ALTO_CK(cudaEventRecord(bt->ev_scan[g], st));
       ALTO_CK(cudaStreamWaitEvent(ts, bt->ev_scan[g], 0));
-    } else if (before_last_tail) {
+      forked = true;
+    } else if (last && before_last_tail) {
       ALTO_CK(cudaEventRecord(before_last_tail, st));
     }
-    ALTO_CK(alto::launch_tail(tail_args(e, bt, d_slots, slot_stride, resp, resp_stride, g * parts, parts), slots, ts));
+    ALTO_CK(alto::launch_tail(tail_args(e, bt, d_slots, slot_stride, resp, resp_stride, o0, parts), slots, ts));
     *launches += 2;
     if (done) ALTO_CK(cudaEventRecord(done[g], ts));
   }
-  if (groups > 1) {  // join the side stream's tails
+  if (forked) {  // join the side stream's tails
     ALTO_CK(cudaEventRecord(bt->ev_join, bt->side));
     ALTO_CK(cudaStreamWaitEvent(st, bt->ev_join, 0));
   }
@@ -757,7 +792,7 @@ bool enqueue_batch_direct(Engine *e, Batch *bt, const uint8_t *d_slots, size_t s
                           uint8_t *resp, size_t resp_stride, bool host_status, bool with_marks) {
   cudaStream_t st = bt->st;
   const Plan p = make_plan(e, slots);
-  const int groups = e->overlap ? column_groups(e, p, e->groups) : 1;
+  const Groups groups = column_groups(e, p, e->overlap ? e->groups : 1);
   const int bp = (int)round_up(slots, 4);
   int launches = 0;
   // timing marks (main batch only): 0 begin | validate | 1 | y split | 2 | pack | 3 | (wait for the query split)
@@ -805,7 +840,8 @@ bool enqueue_batch_direct(Engine *e, Batch *bt, const uint8_t *d_slots, size_t s
     launches += 1;
   }
   ALTO_CK(mark(4));
-  if (!enqueue_scan_tails(e, bt, p, map_q, d_slots, slot_stride, slots, resp, resp_stride, groups, nullptr, &launches,
+  if (!enqueue_scan_tails(e, bt, p, map_q, d_slots, slot_stride, slots, resp, resp_stride, groups, nullptr,
+                          &launches,
                           mk ? mk[5] : nullptr))
     return false;
   ALTO_CK(mark(6));
@@ -959,7 +995,7 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
   cudaStream_t st = bt->st, sc = e->st_copy;
   const size_t nc = cand.size();
   const Plan p = make_plan(e, nc);
-  const int groups = e->overlap ? column_groups(e, p, e->host_groups) : 1;
+  const Groups groups = column_groups(e, p, e->overlap ? e->host_groups : 1, true);
   const int bp = (int)round_up(nc, 4);
   const size_t ybytes = 9 + 4 * e->count;  // header and y keys
   int launches = 0;
@@ -1026,10 +1062,10 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
     status[cand[i]] = bt->h_status[i];
     if (bt->h_status[i] == 0) ok.push_back(i);
   }
-  const size_t gbytes = (size_t)(e->outputs / groups) * e->part_len;
-  for (int g = 0; g < groups; ++g) {
+  for (int g = 0; g < groups.count; ++g) {
     ALTO_H(cudaStreamWaitEvent(sc, e->ev_group[g], 0));
-    const size_t off = (size_t)g * gbytes;
+    const size_t off = (size_t)groups.bounds[g] * e->part_len;
+    const size_t gbytes = (size_t)(groups.bounds[g + 1] - groups.bounds[g]) * e->part_len;
     if (!copy_runs(
             ok.size(), gbytes, [&](size_t k) { return (const void *)(bt->d_resp + ok[k] * e->resp_len + off); },
             [&](size_t k) { return (void *)(out[cand[ok[k]]] + off); }, cudaMemcpyDeviceToHost, sc))
@@ -1041,9 +1077,9 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
   if (stage_ms) {
     float t0, t1, t2, t3;
     ALTO_H(cudaEventElapsedTime(&t0, e->ev_begin, e->ev_keys));                // key upload
-    ALTO_H(cudaEventElapsedTime(&t1, e->ev_status, e->ev_group[groups - 1]));  // query split + scan + tails
+    ALTO_H(cudaEventElapsedTime(&t1, e->ev_status, e->ev_group[groups.count - 1]));  // query split + scan + tails
     ALTO_H(cudaEventElapsedTime(&t2, e->ev_keys, e->ev_pack));                 // key split + pack
-    ALTO_H(cudaEventElapsedTime(&t3, e->ev_group[groups - 1], e->ev_end));     // last download
+    ALTO_H(cudaEventElapsedTime(&t3, e->ev_group[groups.count - 1], e->ev_end));     // last download
     stage_ms[0] = t0;
     stage_ms[1] = t1;
     stage_ms[2] = t2;

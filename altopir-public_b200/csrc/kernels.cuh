@@ -12,27 +12,30 @@ namespace alto {
 // 16-byte aligned.  Status 2 for a flag byte != 0 or a key count != tg * n (src/amx_kernels.cpp:575), 3 for any of
 // the 2 * count y/z key words >= Q (src/amx_kernels.cpp:576-580), else 0.  Query words are not range-checked, as in
 // the reference.  Status 1 (length) is settled by the host before a frame is staged.
-// Rearranges a staged slab (up to 128 rows of `pitch` bytes; nr valid rows of nk valid bytes) into consecutive
-// 128 x 128-byte tiles of one 128-row tile of a tile-contiguous operand: output word i (16 bytes) is row
-// (i / 8) % 128, bytes 16 (i % 8) of tile i / 1024.  Bytes past the valid rows or width are zero.
-__global__ void tile_slab_kernel(const uint8_t *__restrict__ src, size_t pitch, int nr, int nk, size_t words,
-                                 uint8_t *__restrict__ dst) {
+// Rearranges a staged slab into the tile-contiguous layout: the stage holds consecutive 128-row tiles (row tile j in
+// rows [128 j, 128 j + 128), nr valid rows in all, nk valid bytes of `pitch`), and each becomes `tiles` consecutive
+// 128 x 128-byte tiles at dst + (j * kbs + kb0 + t) * 16 KB.  One thread per 16-byte output word; bytes past the
+// valid rows or width are zero.
+__global__ void tile_slab_kernel(const uint8_t *__restrict__ src, size_t pitch, int nr, int nk, int tiles,
+                                 size_t words, uint8_t *__restrict__ dst, size_t kbs, size_t kb0) {
   const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i >= words) return;
-  const int r = (int)((i >> 3) & 127);
-  const size_t k = (i >> 10) * 128 + (i & 7) * 16;
+  const size_t per = (size_t)tiles * 1024;  // words per row tile
+  const size_t j = i / per, rest = i - j * per;
+  const int r = (int)((rest >> 3) & 127);
+  const size_t row = j * 128 + r, k = (rest >> 10) * 128 + (rest & 7) * 16;
   uint4 v = make_uint4(0, 0, 0, 0);
-  if (r < nr && k < (size_t)nk) {
-    const uint8_t *p = src + (size_t)r * pitch + k;
+  if (row < (size_t)nr && k < (size_t)nk) {
+    const uint8_t *p = src + row * pitch + k;
     if (k + 16 <= (size_t)nk) {
       v = *reinterpret_cast<const uint4 *>(p);
     } else {
       uint8_t b[16] = {};
-      for (size_t j = 0; k + j < (size_t)nk; ++j) b[j] = p[j];
+      for (size_t q = 0; k + q < (size_t)nk; ++q) b[q] = p[q];
       memcpy(&v, b, 16);
     }
   }
-  reinterpret_cast<uint4 *>(dst)[i] = v;
+  reinterpret_cast<uint4 *>(dst)[((j * kbs + kb0) << 10) + rest] = v;
 }
 
 __global__ void validate_kernel(const uint8_t *__restrict__ slots, size_t stride, size_t lead, size_t count,

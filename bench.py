@@ -386,6 +386,9 @@ def main_ours(a):
     # ---- the plain path: one query per launch, each waited for
     lat = []
     one = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for i in range(max(3, a.warmup)):  # untimed: the first single-query launches load their kernels
+        e.enqueue_device(slots[i % B].data_ptr(), stride, 1, d_out[i % B].data_ptr(), rl, None)
+    e.sync()
     barrier()
     for i in range(a.plain_queries):
         c = i % B

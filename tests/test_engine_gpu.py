@@ -234,3 +234,18 @@ def test_every_schedule_returns_identical_bytes(gpu, svc, eng, monkeypatch):
             want = host
         assert np.array_equal(host, want), (overlap, groups, host_groups)
         e.close()
+
+
+def test_record_count_off_the_tile_grid_matches_oracle(gpu, oracle, svc, eng):
+    # 2112 records: the last 128-record block of the tiled database is half padding, which must read as zero.  The
+    # service layer only takes powers of two (as the reference's does); the engine's C ABI takes any multiple of 64.
+    p = svc.Params(2112, 4096)
+    st = svc.SyntheticState.make(p, seed=51, full_prefix=True)
+    e = eng.Engine.from_state(st, threads=svc.threads())
+    req = svc.synthetic_requests(p, 9, seed=52)
+    frames_ = [req[i] for i in range(9)]
+    n, status, out = _answer(e, frames_)
+    assert n == 9 and (status == 0).all()
+    r, ost, oout = oracle.answer(st, frames_)
+    assert np.array_equal(out, oout)
+    e.close()
