@@ -144,14 +144,15 @@ def int8_cublas_tops(torch):
 
 
 def traffic_from_profile(kernel, rows, record_bytes, batch):
-    """DRAM bytes per launch of `kernel` from the committed ncu capture (profiles/ncu_traffic.json), which covers the
-    default workload only; None for any other configuration."""
+    """DRAM bytes per batch of `kernel` (summed over its launches in one batch, the unit its CUDA-event timing uses)
+    from the committed ncu capture (profiles/ncu_traffic.json), which covers the default workload only; None for any
+    other configuration."""
     if (rows, record_bytes, batch) != (32768, 32768, 128):
         return None
     path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     try:
         with open(path) as f:
-            return json.load(f).get(kernel, {}).get("dram_bytes_per_launch")
+            return json.load(f).get(kernel, {}).get("dram_bytes_per_batch")
     except OSError:
         return None
 
