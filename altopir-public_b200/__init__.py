@@ -56,6 +56,9 @@ def _declare(L):
         "alto_server_wait": (I, [P, c.c_longlong, P, S, I, c.POINTER(c.c_double)]),
         "alto_server_stats": (I, [P, c.POINTER(c.c_double), S]),
         "alto_server_free": (None, [P]),
+        "alto_engine_new_empty": (P, [S, S, P, S, S, PP, S, S, U64, I, PP, P, U64, I]),
+        "alto_engine_load_records": (I, [P, P, S, S, S]),
+        "alto_engine_load_file": (I, [P, c.c_char_p, S]),
         "alto_synthetic_db_col": (None, [P, S, S, S, S, I]),
         "alto_synthetic_db_col_device": (I, [P, S, S, S, S]),
         "alto_fill_uniform_u32": (None, [P, S, U64, U64, I]),
@@ -81,7 +84,8 @@ EXPORTS = (
     "alto_engine_free", "alto_request_len", "alto_response_len", "alto_answer", "alto_last_error",
     "alto_answer_device", "alto_last_launches", "alto_enqueue_device", "alto_engine_sync", "alto_engine_stream",
     "alto_kernel_times", "alto_engine_set_graphs", "alto_engine_set_tuning", "alto_answer_device_noalloc", "alto_server_new", "alto_server_new_loopback",
-    "alto_server_submit", "alto_server_wait", "alto_server_stats", "alto_server_free", "alto_synthetic_db_col", "alto_synthetic_db_col_device",
+    "alto_server_submit", "alto_server_wait", "alto_server_stats", "alto_server_free", "alto_engine_new_empty",
+    "alto_engine_load_records", "alto_engine_load_file", "alto_synthetic_db_col", "alto_synthetic_db_col_device",
     "alto_fill_uniform_u32", "alto_fill_uniform_u64", "alto_fill_bytes", "alto_synthetic_request",
     "alto_pack_encode", "alto_rescale_digest",
 )

@@ -1109,12 +1109,50 @@ int sw_amx_init(void) {
   return 0;
 }
 
-void *alto_engine_new(const uint8_t *db_col, const uint8_t *db_tiled, size_t ld, size_t rows, size_t cols,
-                      const int8_t *ub, size_t n, size_t tg, const uint8_t *const *prefix, size_t part_len,
-                      size_t row1_off, uint64_t q1, int q1_bits, const uint64_t *const *that,
-                      const uint64_t *inv_table, uint64_t q, int threads) {
+}  // extern "C"
+
+namespace {
+
+// Loads records [first, first + count) from a record-major host buffer (record i at records + (i - first) * pitch,
+// cols bytes each) into the database tiles, through a 64 MB device staging buffer: per pass, whole 128-record
+// blocks of the tile grid (the first and last may be partly covered, their other records kept).
+bool load_records(Engine *e, const uint8_t *records, size_t pitch, size_t first, size_t count) {
+  ALTO_CK(cudaStreamSynchronize(e->main.st));  // batches already enqueued read the database
+  const size_t per = std::max<size_t>(128, (size_t(64) << 20) / e->cols / 128 * 128);  // records per pass
+  uint8_t *stage = nullptr;
+  ALTO_CK(cudaMalloc(&stage, per * e->cols));
+  bool ok = true;
+  const size_t end = first + count;
+  for (size_t a = first / 128 * 128; a < end && ok; a += per) {
+    const size_t lo = std::max(a, first), hi = std::min(a + per, end);
+    cudaError_t err = cudaMemcpy2D(stage + (lo - a) * e->cols, e->cols, records + (lo - first) * pitch, pitch,
+                                   e->cols, hi - lo, cudaMemcpyHostToDevice);
+    if (err == cudaSuccess) {
+      const dim3 grid((unsigned)((hi - a + 127) / 128), (unsigned)e->db_mts);
+      alto::records_to_tiles_kernel<<<grid, 256>>>(stage, e->cols, a, lo, hi, e->d_db, e->db_kbs, e->cols);
+      err = cudaGetLastError();
+    }
+    if (err != cudaSuccess) {
+      set_error("database load", err);
+      ok = false;
+    }
+  }
+  const cudaError_t sync = cudaStreamSynchronize(0);
+  if (ok && sync != cudaSuccess) {
+    set_error("database load", sync);
+    ok = false;
+  }
+  cudaFree(stage);
+  return ok;
+}
+
+// The engine with the database db_col (column order, row pitch ld), or with a zero database to be loaded later
+// (alto_engine_load_records) when db_col is NULL.
+void *create_engine(const uint8_t *db_col, size_t ld, size_t rows, size_t cols, const int8_t *ub, size_t n,
+                    size_t tg, const uint8_t *const *prefix, size_t part_len, size_t row1_off, uint64_t q1,
+                    int q1_bits, const uint64_t *const *that, const uint64_t *inv_table, uint64_t q, int threads) {
   // The reference's checks (src/amx_kernels.cpp:551-552), then this engine's own limits.
-  if (!db_col || !db_tiled || !ub || !prefix || !that || !inv_table || q != alto::kQ || !n || n > 4096 || n % 16 ||
+  if (!ub || !prefix || !that || !inv_table || q != alto::kQ || !n || n > 4096 || n % 16 ||
       cols % n || rows % 64 || cols % 32 || threads <= 0 || (tg * n) % 128) {
     set_error("unsupported engine configuration");
     return nullptr;
@@ -1177,7 +1215,9 @@ void *alto_engine_new(const uint8_t *db_col, const uint8_t *db_tiled, size_t ld,
   e->ub_kbs = e->count / 128;
   e->ub_mts = (4 * cols + 127) / 128;
   if ((err = cudaMalloc(&e->d_db, e->db_mts * e->db_kbs * 16384)) != cudaSuccess) return fail("database", err);
-  if (!upload_tiled(e->d_db, db_col, ld, cols, rows, e->db_kbs, e->db_mts)) {
+  if (!db_col) {
+    if ((err = cudaMemset(e->d_db, 0, e->db_mts * e->db_kbs * 16384)) != cudaSuccess) return fail("database", err);
+  } else if (!upload_tiled(e->d_db, db_col, ld, cols, rows, e->db_kbs, e->db_mts)) {
     destroy(e);
     return nullptr;
   }
@@ -1213,6 +1253,69 @@ void *alto_engine_new(const uint8_t *db_col, const uint8_t *db_tiled, size_t ld,
   resident_pairs();  // occupancy query outside any stream capture
   load_tuning(e);
   return e;
+}
+
+}  // namespace
+
+extern "C" {
+
+void *alto_engine_new(const uint8_t *db_col, const uint8_t *db_tiled, size_t ld, size_t rows, size_t cols,
+                      const int8_t *ub, size_t n, size_t tg, const uint8_t *const *prefix, size_t part_len,
+                      size_t row1_off, uint64_t q1, int q1_bits, const uint64_t *const *that,
+                      const uint64_t *inv_table, uint64_t q, int threads) {
+  if (!db_col || !db_tiled) {  // src/amx_kernels.cpp:551
+    set_error("unsupported engine configuration");
+    return nullptr;
+  }
+  return create_engine(db_col, ld, rows, cols, ub, n, tg, prefix, part_len, row1_off, q1, q1_bits, that, inv_table,
+                       q, threads);
+}
+
+void *alto_engine_new_empty(size_t rows, size_t cols, const int8_t *ub, size_t n, size_t tg,
+                            const uint8_t *const *prefix, size_t part_len, size_t row1_off, uint64_t q1, int q1_bits,
+                            const uint64_t *const *that, const uint64_t *inv_table, uint64_t q, int threads) {
+  return create_engine(nullptr, rows, rows, cols, ub, n, tg, prefix, part_len, row1_off, q1, q1_bits, that, inv_table,
+                       q, threads);
+}
+
+int alto_engine_load_records(void *p, const uint8_t *records, size_t pitch, size_t first, size_t count) {
+  Engine *e = static_cast<Engine *>(p);
+  if (!e || (!records && count) || pitch < e->cols || first > e->rows || count > e->rows - first) {
+    set_error("alto_engine_load_records: bad arguments");
+    return -1;
+  }
+  if (!count) return 0;
+  if (cudaSetDevice(e->dev) != cudaSuccess || !load_records(e, records, pitch, first, count)) return -4;
+  return 0;
+}
+
+int alto_engine_load_file(void *p, const char *path, size_t num_real_rows) {
+  Engine *e = static_cast<Engine *>(p);
+  if (!e || !path || num_real_rows > e->rows) {
+    set_error("alto_engine_load_file: bad arguments");
+    return -1;
+  }
+  FILE *f = fopen(path, "rb");
+  if (!f) {
+    set_error(std::string("alto_engine_load_file: cannot open ") + path);
+    return -2;
+  }
+  // whole blocks of 128 records per read (about 4 MB per 128 records of 32 KB), at most 64 MB
+  const size_t block = std::max<size_t>(128, (size_t(64) << 20) / e->cols / 128 * 128);
+  std::vector<uint8_t> buf(block * e->cols);
+  int rc = 0;
+  if (cudaSetDevice(e->dev) != cudaSuccess) rc = -4;
+  for (size_t r0 = 0; r0 < num_real_rows && rc == 0; r0 += block) {
+    const size_t nr = std::min(block, num_real_rows - r0);
+    if (fread(buf.data(), e->cols, nr, f) != nr) {
+      set_error(std::string("alto_engine_load_file: short read in ") + path);
+      rc = -2;
+    } else if (!load_records(e, buf.data(), e->cols, r0, nr)) {
+      rc = -4;
+    }
+  }
+  fclose(f);
+  return rc;
 }
 
 void alto_engine_free(void *p) { destroy(static_cast<Engine *>(p)); }

@@ -38,6 +38,44 @@ __global__ void tile_slab_kernel(const uint8_t *__restrict__ src, size_t pitch, 
   reinterpret_cast<uint4 *>(dst)[((j * kbs + kb0) << 10) + rest] = v;
 }
 
+// Transposes record-major records into the database's tile layout.  The stage holds records [a, a + S) (record i at
+// stage + (i - a) * cols); records [lo, hi) are valid.  Block (x, y) fills tile (mt = y, kb = a / 128 + x): tile
+// row r is database column 128 mt + r, byte k of it record 128 kb + k.  Records of the tile outside [lo, hi) keep
+// their bytes; columns past `cols` are left alone (they stay zero).
+__global__ void __launch_bounds__(256) records_to_tiles_kernel(const uint8_t *__restrict__ stage, size_t cols, size_t a,
+                                                               size_t lo, size_t hi, uint8_t *__restrict__ db,
+                                                               size_t kbs, size_t ncols) {
+  __shared__ __align__(16) uint8_t t[128][144];  // [column in tile][record in tile], rows padded to 144 bytes
+  const size_t kb = a / 128 + blockIdx.x, mt = blockIdx.y;
+  const size_t rec0 = kb * 128, col0 = mt * 128;
+  const size_t klo = lo > rec0 ? lo - rec0 : 0, khi = hi < rec0 + 128 ? hi - rec0 : 128;
+  // load: 128 records x 8 chunks of 16 bytes, transposed into shared memory byte by byte
+  for (int i = threadIdx.x; i < 1024; i += 256) {
+    const int k = i >> 3, c16 = i & 7;
+    const size_t col = col0 + c16 * 16;
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if ((size_t)k >= klo && (size_t)k < khi && col < ncols)
+      v = *reinterpret_cast<const uint4 *>(stage + (rec0 + k - a) * cols + col);
+    const uint8_t *b = reinterpret_cast<const uint8_t *>(&v);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) t[c16 * 16 + j][k] = b[j];
+  }
+  __syncthreads();
+  uint8_t *tile = db + (mt * kbs + kb) * 16384;
+  if (klo == 0 && khi == 128) {
+    for (int i = threadIdx.x; i < 1024; i += 256) {  // whole tile: 16-byte stores
+      const int r = i >> 3, k16 = i & 7;
+      if (col0 + r < ncols)
+        *reinterpret_cast<uint4 *>(tile + r * 128 + k16 * 16) = *reinterpret_cast<const uint4 *>(&t[r][k16 * 16]);
+    }
+  } else {
+    for (int i = threadIdx.x; i < 128 * 128; i += 256) {  // part of the records: byte stores of those only
+      const int r = i >> 7, k = i & 127;
+      if ((size_t)k >= klo && (size_t)k < khi && col0 + r < ncols) tile[r * 128 + k] = t[r][k];
+    }
+  }
+}
+
 __global__ void validate_kernel(const uint8_t *__restrict__ slots, size_t stride, size_t lead, size_t count,
                                 size_t rows, int *__restrict__ status) {
   (void)rows;

@@ -2,6 +2,7 @@
 TiledDb, build_packing_matrix and Engine, all calling the C ABI of libaltopir_gpu.so."""
 import ctypes
 import enum
+import os
 
 import numpy as np
 
@@ -78,6 +79,35 @@ class Engine:
                                          part_len, row1_off, q1, q1_bits, _ptrs(that64), _p(inv), q, threads)
         if not self.ptr:
             raise EngineError(f"unsupported engine configuration: {last_error()}")
+
+    @classmethod
+    def empty(cls, rows, cols, ub, n, tg, prefixes, row1_off, q1, q1_bits, that, inv_table, q=Q, threads=1):
+        """alto_engine_new_empty: the engine without its database, which starts as zeros and is filled with
+        load_records or load_file (the reference server's streaming reader, src/server.rs:380-500)."""
+        assert ub.size == 4 * tg * n * cols and len(prefixes) == cols // n and len(that) == cols // n
+        self = cls.__new__(cls)
+        pre = [np.ascontiguousarray(p, dtype=np.uint8) for p in prefixes]
+        that64 = [np.ascontiguousarray(t, dtype=np.uint64) for t in that]
+        inv = np.ascontiguousarray(inv_table, dtype=np.uint64)
+        ub = np.ascontiguousarray(ub)
+        self.ptr = lib().alto_engine_new_empty(rows, cols, _p(ub), n, tg, _ptrs(pre), pre[0].size, row1_off, q1,
+                                               q1_bits, _ptrs(that64), _p(inv), q, threads)
+        if not self.ptr:
+            raise EngineError(f"unsupported engine configuration: {last_error()}")
+        return self
+
+    def load_records(self, records, first):
+        """alto_engine_load_records: records is a (count, cols) uint8 array of consecutive records from `first`."""
+        records = np.ascontiguousarray(records, dtype=np.uint8)
+        r = lib().alto_engine_load_records(self.ptr, _p(records), records.shape[1], first, records.shape[0])
+        if r < 0:
+            raise EngineError(f"engine error {r}: {last_error()}")
+
+    def load_file(self, path, num_real_rows):
+        """alto_engine_load_file: the first num_real_rows records of a flat record-major database file."""
+        r = lib().alto_engine_load_file(self.ptr, os.fsencode(path), num_real_rows)
+        if r < 0:
+            raise EngineError(f"engine error {r}: {last_error()}")
 
     @staticmethod
     def from_state(st, threads=1, tile=True):

@@ -122,6 +122,15 @@ def synthetic_record(row, nbytes):
     return (z % np.uint64(65535)).astype("<u2").view(np.uint8)
 
 
+def write_record_file(path, db_col, num_real_rows, block=4096):
+    """Writes the first num_real_rows records of a column-order database (db_col[col][r]) as the reference's on-disk
+    database: records one after another, each the record's bytes in column order (the input of its streaming reader,
+    src/server.rs:380-500)."""
+    with open(path, "wb") as f:
+        for r0 in range(0, num_real_rows, block):
+            f.write(np.ascontiguousarray(db_col[:, r0:min(r0 + block, num_real_rows)].T).tobytes())
+
+
 def synthetic_db_col(rows, cols, col0=0, ld=None):
     """The server's column-order database of the synthetic records: db[col][row] = record(row)[col0 + col]
     (src/service.rs:64-78 followed by the column-major transpose of src/server.rs:251-366)."""

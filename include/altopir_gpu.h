@@ -33,9 +33,9 @@ void *sw_alloc(size_t bytes);
 void sw_free(void *p);
 
 /* Replaces sw_tile_db (src/amx_kernels.cpp:138-149).  Copies the k x m column-order database db[col * ld + r]
- * into dst as a compact column-order matrix dst[col * k + r] (k records per column, no padding).  This is the
- * engine's own tiled layout: the device reads it in 128-record x 128-column boxes through TMA, so no further
- * host-side tiling exists.  Uses `threads` host threads. */
+ * into dst as a compact column-order matrix dst[col * k + r] (k records per column, no padding).  The engine does
+ * not read this copy: alto_engine_new builds its own tiles of 128 columns x 128 records in device memory from
+ * db_col.  Kept so that callers written for the reference link unchanged.  Uses `threads` host threads. */
 void sw_tile_db(uint8_t *dst, const uint8_t *db, size_t ld, size_t k, size_t m, int threads);
 
 /* Replaces sw_pack_build (src/amx_kernels.cpp:311-341).  Folds the InspiRING automorphisms into the dense packing
@@ -176,6 +176,26 @@ int alto_server_wait(void *server, long long ticket, uint8_t *out, size_t out_le
                      double *latency_ms);
 int alto_server_stats(void *server, double *out, size_t n);
 void alto_server_free(void *server);
+
+/* A database too large to hold in host memory in column order, or stored on disk record by record, is loaded
+ * straight into the engine's device tiles instead of through alto_engine_new's db_col (the counterpart of the
+ * reference server's streaming reader, src/server.rs:380-500, which transposes a record-major file into the
+ * column-order buffer).
+ * alto_engine_new_empty: alto_engine_new without the database (same checks, same copies of the other state); the
+ *   database starts as zeros, as the reference's padding records are.
+ * alto_engine_load_records: copies records [first, first + count) -- record i at records + (i - first) * pitch,
+ *   cols bytes each, pitch >= cols -- into the engine's database, transposing them on the device.  Any run of
+ *   records, in any order; records not loaded keep their bytes.  Waits for the engine's enqueued batches first;
+ *   must not overlap another call on the same engine.  0, -1 for bad arguments (first + count > rows, ...), -4 for
+ *   a device failure.
+ * alto_engine_load_file: loads the first num_real_rows records of a flat record-major file (num_real_rows records
+ *   of cols bytes each, the reference's on-disk database) in 64 MB reads; the rest stay zero.  0, -1 for bad
+ *   arguments, -2 when the file cannot be opened or is short, -4 for a device failure. */
+void *alto_engine_new_empty(size_t rows, size_t cols, const int8_t *ub, size_t n, size_t tg,
+                            const uint8_t *const *prefix, size_t part_len, size_t row1_off, uint64_t q1, int q1_bits,
+                            const uint64_t *const *that, const uint64_t *inv_table, uint64_t q, int threads);
+int alto_engine_load_records(void *engine, const uint8_t *records, size_t pitch, size_t first, size_t count);
+int alto_engine_load_file(void *engine, const char *path, size_t num_real_rows);
 
 /* Deterministic synthetic inputs (test and benchmark data; not part of the answer path).
  * alto_synthetic_db_col: db[(col - col0) * ld + r] = byte col of the reference's synthetic record r

@@ -1,0 +1,69 @@
+"""Loading the database straight into the engine's device tiles (alto_engine_new_empty, alto_engine_load_records,
+alto_engine_load_file): the engine answers exactly as one built from the column-order database, for records loaded
+in uneven pieces that straddle the 128-record tile grid, and for a record-major file shorter than the database (the
+reference's streaming reader pads the remaining records with zeros, src/server.rs:380-500)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _empty_like(eng, st):
+    p = st.p
+    return eng.Engine.empty(p.rows, p.record_bytes, st.ub, p.n, p.tg, st.prefixes, p.row1_off, 1 << p.q1_bits,
+                            p.q1_bits, st.that, st.inv_table)
+
+
+def _answer(e, frames):
+    b = len(frames)
+    out = np.zeros((b, e.response_len()), dtype=np.uint8)
+    status = np.full(b, -1, dtype=np.int32)
+    r, _ = e.answer([frames[i] for i in range(b)], out, status)
+    assert r == b
+    return out
+
+
+def test_records_loaded_in_pieces_answer_like_the_column_order_database(gpu, svc, eng):
+    p = svc.params(4096, 8192)
+    st = svc.SyntheticState.make(p, seed=91, full_prefix=True)
+    frames = svc.synthetic_requests(p, 6, seed=92)
+    full = eng.Engine.from_state(st)
+    want = _answer(full, frames)
+    full.close()
+    e = _empty_like(eng, st)
+    assert e.request_len() == svc.request_len(p)
+    for a, b in ((3000, 4096), (0, 1000), (1000, 1100), (1100, 3000)):  # uneven, out of order, off the tile grid
+        e.load_records(st.db_col[:, a:b].T, a)
+    assert np.array_equal(_answer(e, frames), want)
+    # reloading a run with other bytes changes the answer; loading the originals back restores it
+    e.load_records(np.zeros((300, p.record_bytes), dtype=np.uint8), 2000)
+    assert not np.array_equal(_answer(e, frames), want)
+    e.load_records(st.db_col[:, 2000:2300].T, 2000)
+    assert np.array_equal(_answer(e, frames), want)
+    with pytest.raises(eng.EngineError):
+        e.load_records(st.db_col[:, :200].T, 4000)  # runs past the database
+    e.close()
+
+
+def test_record_file_shorter_than_the_database_reads_as_zero_padded(gpu, oracle, svc, eng, tmp_path):
+    p = svc.params(4096, 8192)
+    st = svc.SyntheticState.make(p, seed=93, full_prefix=True)
+    real = 2500
+    path = tmp_path / "db.bin"
+    svc.write_record_file(path, st.db_col, real)
+    assert path.stat().st_size == real * p.record_bytes
+    e = _empty_like(eng, st)
+    e.load_file(path, real)
+    frames = svc.synthetic_requests(p, 5, seed=94)
+    got = _answer(e, frames)
+    st.db_col[:, real:] = 0  # what the reference's reader leaves past the real records
+    full = eng.Engine.from_state(st)
+    assert np.array_equal(got, _answer(full, frames))
+    full.close()
+    r, status, oout = oracle.answer(st, [frames[i] for i in range(5)])
+    assert np.array_equal(got, oout)
+    with pytest.raises(eng.EngineError):
+        e.load_file(tmp_path / "missing.bin", real)
+    with pytest.raises(eng.EngineError):
+        e.load_file(path, real + 128)  # the file is short
+    e.close()
