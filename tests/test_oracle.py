@@ -145,3 +145,18 @@ def test_reference_engine_agrees_when_available(oracle, svc):
     for m in methods:
         rr, rs, rout, _ = ref.answer(frames_, m)
         assert rr == r and np.array_equal(rs, status) and np.array_equal(rout, out)
+
+
+def test_pack_build_at_the_scheme_shape_matches_oracle(oracle, svc, eng):
+    # n = 2048, tg = 4 and the scheme's n/2 - 1 automorphisms, with 64-bit sums that wrap
+    n, tg, rho = 2048, 4, 2
+    it = n // 2 - 1
+    bt = [svc.uniform_u64(it * tg * n, 1 << 32, 900 + o) << np.uint64(31) for o in range(rho)]
+    btb = [svc.uniform_u64(it * tg * n, 1 << 32, 950 + o) << np.uint64(30) for o in range(rho)]
+    tables = svc.uniform_u32(n * n, n, 990)
+    gen_pows = np.array([pow(5, i, 2 * n) for i in range(it)], dtype=np.uint32)
+    ub = np.zeros(4 * tg * n * rho * n, dtype=np.int8)
+    eng.build_packing_matrix(ub, bt, btb, tables, gen_pows, it, tg, n, threads=4)
+    planes = ub.view(np.uint8).reshape(rho * n, 4, tg * n).astype(np.uint32)
+    mine = planes[:, 0] | (planes[:, 1] << 8) | (planes[:, 2] << 16) | (planes[:, 3] << 24)
+    assert np.array_equal(mine, oracle.pack_build(bt, btb, tables, gen_pows, it, tg, n))
