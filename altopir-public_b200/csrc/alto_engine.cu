@@ -784,10 +784,10 @@ bool enqueue_scan_tails(Engine *e, Batch *bt, const Plan &p, const CUtensorMap &
 
 // Enqueues the answer path for `slots` staged frames on the batch's stream: validate, key limb split, pack GEMM,
 // query limb split, scan GEMM and tail.  Statuses go to d_status (and to the pinned host copy when host_status);
-// responses of valid frames to resp + slot * resp_stride.  With the overlapped schedule the query limb split and the
-// zeroing of the scan sums run on the side stream beside validation and the pack, and the tails of all column groups
-// but the last beside the scan (enqueue_scan_tails); the side stream forks from and joins back into the batch's
-// stream, so the batch is complete when its stream passes it.
+// responses of valid frames to resp + slot * resp_stride.  With the overlapped schedule validation, the query limb
+// split and the zeroing of the scan sums run on the side stream beside the key limb split and the pack, and the
+// tails of all column groups but the last beside the scan (enqueue_scan_tails); the side stream forks from and joins
+// back into the batch's stream, so the batch is complete when its stream passes it.
 bool enqueue_batch_direct(Engine *e, Batch *bt, const uint8_t *d_slots, size_t slot_stride, size_t slots,
                           uint8_t *resp, size_t resp_stride, bool host_status, bool with_marks) {
   cudaStream_t st = bt->st;
@@ -795,8 +795,9 @@ bool enqueue_batch_direct(Engine *e, Batch *bt, const uint8_t *d_slots, size_t s
   const Groups groups = column_groups(e, p, e->overlap ? e->groups : 1);
   const int bp = (int)round_up(slots, 4);
   int launches = 0;
-  // timing marks (main batch only): 0 begin | validate | 1 | y split | 2 | pack | 3 | (wait for the query split)
-  // | 4 | scan (with all tails but the last beside it) | 5 | last tail | 6
+  // timing marks (main batch only): 0 begin | validate (one stream only) | 1 | y split | 2 | pack | 3 | (wait for
+  // the side stream) | 4 | scan (with all tails but the last beside it) | 5 | last tail | 6.  With two streams the
+  // intervals are the exposed times: validation and the query split run beside the key split and the pack.
   cudaEvent_t *mk = nullptr;
   if (bt->timing && with_marks) {
     int set = 0;
@@ -805,19 +806,24 @@ bool enqueue_batch_direct(Engine *e, Batch *bt, const uint8_t *d_slots, size_t s
   }
   auto mark = [&](int i) { return mk ? cudaEventRecord(mk[i], st) : cudaSuccess; };
   ALTO_CK(mark(0));
+  // validation (its statuses are needed by the tails only) and the query limb split: on the side stream when the
+  // schedule has two, joined before the scan
+  cudaStream_t vs = st;
   if (e->overlap) {
+    vs = bt->side;
     ALTO_CK(cudaEventRecord(bt->ev_fork, st));
-    ALTO_CK(cudaStreamWaitEvent(bt->side, bt->ev_fork, 0));
-    if (!enqueue_query_split(e, bt, d_slots, slot_stride, slots, bt->side)) return false;
-    launches += 1;
-    ALTO_CK(cudaEventRecord(bt->ev_qready, bt->side));
+    ALTO_CK(cudaStreamWaitEvent(vs, bt->ev_fork, 0));
   }
-
-  alto::validate_kernel<<<(unsigned)slots, 256, 0, st>>>(d_slots, slot_stride, kSlotLead, e->count, e->rows,
+  alto::validate_kernel<<<(unsigned)slots, 256, 0, vs>>>(d_slots, slot_stride, kSlotLead, e->count, e->rows,
                                                          bt->d_status);
   ++launches;
   ALTO_CK(cudaGetLastError());
-  if (host_status) ALTO_CK(cudaMemcpyAsync(bt->h_status, bt->d_status, slots * sizeof(int), cudaMemcpyDeviceToHost, st));
+  if (host_status) ALTO_CK(cudaMemcpyAsync(bt->h_status, bt->d_status, slots * sizeof(int), cudaMemcpyDeviceToHost, vs));
+  if (e->overlap) {
+    if (!enqueue_query_split(e, bt, d_slots, slot_stride, slots, vs)) return false;
+    launches += 1;
+    ALTO_CK(cudaEventRecord(bt->ev_qready, vs));
+  }
   ALTO_CK(mark(1));
 
   CUtensorMap map_q, map_y;
