@@ -922,9 +922,9 @@ bool copy_runs(size_t items, size_t width, SrcAt src_at, DstAt dst_at, cudaMemcp
 
 // Waits for the engine's stream, folds pending timing marks into the totals and checks (then clears) the device
 // error word.
-bool sync_engine(Engine *e) {
-  ALTO_CK(cudaMemcpyAsync(e->main.h_err, e->main.d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->main.st));
-  ALTO_CK(cudaStreamSynchronize(e->main.st));
+// After the main batch's stream has passed a copy of its error word into the pinned mirror: false (and the word
+// reset) when a kernel wait timed out.
+bool check_error_word(Engine *e) {
   const uint32_t err = *e->main.h_err;
   if (err) {
     ALTO_CK(cudaMemsetAsync(e->main.d_err, 0, sizeof(uint32_t), e->main.st));
@@ -935,6 +935,12 @@ bool sync_engine(Engine *e) {
     return false;
   }
   return accumulate_pending(e);
+}
+
+bool sync_engine(Engine *e) {
+  ALTO_CK(cudaMemcpyAsync(e->main.h_err, e->main.d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->main.st));
+  ALTO_CK(cudaStreamSynchronize(e->main.st));
+  return check_error_word(e);
 }
 
 bool finish(Engine *e, double *stage_ms) {
@@ -1058,6 +1064,8 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
   if (!enqueue_scan_tails(e, bt, p, map_q, bt->d_req, e->slot_stride, nc, bt->d_resp, e->resp_len, groups,
                           e->ev_group, &launches))
     return -4;
+  // the error word comes back behind the last tail, so the final synchronisation covers it
+  ALTO_H(cudaMemcpyAsync(bt->h_err, bt->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   e->last_launches = launches;
 
   // statuses come back as soon as validation is done; then each group's valid responses download on the copy
@@ -1079,7 +1087,8 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
   }
   ALTO_H(cudaEventRecord(e->ev_end, sc));
   ALTO_H(cudaStreamSynchronize(sc));
-  if (!sync_engine(e)) return -4;
+  ALTO_H(cudaStreamSynchronize(st));
+  if (!check_error_word(e)) return -4;
   if (stage_ms) {
     float t0, t1, t2, t3;
     ALTO_H(cudaEventElapsedTime(&t0, e->ev_begin, e->ev_keys));                // key upload

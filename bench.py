@@ -260,12 +260,16 @@ def main_serve(a):
     st.ub = None
     frames = svc.synthetic_requests(p, a.serve_clients, seed=2024)
     rates = [float(x) for x in a.serve.split(",")]
+    print(f"serve: engine and {a.serve_clients} frames ready", file=sys.stderr, flush=True)
     rows = []
     for label, mb in (("batched", a.max_batch), ("plain", 1)):
         s = srv.Server(e, max_batch=mb, queue_cap=max(4 * a.max_batch, 4096), slots=3)
         for rate in rates:
             s.stats()
+            t0 = time.time()
             res, offered, elapsed = srv.poisson_load(s, frames, rate, a.serve_seconds, seed=int(rate), clients=8)
+            print(f"serve {label} {rate:g} QPS offered: {offered} requests in {time.time() - t0:.1f} s",
+                  file=sys.stderr, flush=True)
             lat = sorted(r[3] * 1e3 for r in res if r[1] == 0)
             ok = len(lat)
             pct = lambda q: lat[min(len(lat) - 1, int(q * len(lat)))] if lat else None
