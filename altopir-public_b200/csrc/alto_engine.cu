@@ -238,7 +238,7 @@ struct Engine {
   uint32_t *d_that = nullptr, *d_tw = nullptr;
   Batch main;
   // per call: before the uploads, after the downloads; the query words upload on st_copy
-  cudaEvent_t ev_begin = nullptr, ev_end = nullptr, ev_keys = nullptr, ev_queries = nullptr;
+  cudaEvent_t ev_begin = nullptr, ev_end = nullptr, ev_keys = nullptr, ev_queries = nullptr, ev_zkeys = nullptr;
   cudaStream_t st_copy = nullptr;
   // host pipeline of alto_answer: keys uploaded, pack done, statuses ready, each column group's tail done
   cudaEvent_t ev_pack = nullptr, ev_status = nullptr, ev_group[8] = {};
@@ -396,7 +396,7 @@ void destroy(Engine *e) {
   cudaFree(e->d_that);
   cudaFree(e->d_tw);
   if (e->st_copy) cudaStreamSynchronize(e->st_copy);
-  for (cudaEvent_t ev : {e->ev_begin, e->ev_end, e->ev_keys, e->ev_queries, e->ev_pack, e->ev_status})
+  for (cudaEvent_t ev : {e->ev_begin, e->ev_end, e->ev_keys, e->ev_queries, e->ev_zkeys, e->ev_pack, e->ev_status})
     if (ev) cudaEventDestroy(ev);
   for (cudaEvent_t ev : e->ev_group)
     if (ev) cudaEventDestroy(ev);
@@ -752,8 +752,8 @@ bool enqueue_query_split(const Engine *e, const Batch *bt, const uint8_t *d_slot
 // CTAs be placed first); `done[g]`, when given, is recorded after the tail of group g.
 bool enqueue_scan_tails(Engine *e, Batch *bt, const Plan &p, const CUtensorMap &map_q, const uint8_t *d_slots,
                         size_t slot_stride, size_t slots, uint8_t *resp, size_t resp_stride, const Groups &gr,
-                        const cudaEvent_t *done, int *launches,
-                        cudaEvent_t before_last_tail = nullptr) {
+                        const cudaEvent_t *done, int *launches, cudaEvent_t before_last_tail = nullptr,
+                        cudaEvent_t last_tail_after = nullptr) {
   cudaStream_t st = bt->st;
   bool forked = false;
   for (int g = 0; g < gr.count; ++g) {
@@ -771,6 +771,7 @@ bool enqueue_scan_tails(Engine *e, Batch *bt, const Plan &p, const CUtensorMap &
     } else if (last && before_last_tail) {
       ALTO_CK(cudaEventRecord(before_last_tail, st));
     }
+    if (last && last_tail_after) ALTO_CK(cudaStreamWaitEvent(st, last_tail_after, 0));
     ALTO_CK(alto::launch_tail(tail_args(e, bt, d_slots, slot_stride, resp, resp_stride, o0, parts), slots, ts));
     *launches += 2;
     if (done) ALTO_CK(cudaEventRecord(done[g], ts));
@@ -1026,12 +1027,20 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
     return -4;
   ALTO_H(cudaEventRecord(e->ev_keys, st));
   ALTO_H(cudaStreamWaitEvent(sc, e->ev_keys, 0));
+  // then the query words (the scan's input) and last the z keys, which only validation and the tails read
+  const size_t zbytes = 4 * e->count, qoff = ybytes + zbytes;
   if (!copy_runs(
-          nc, e->want - ybytes, [&](size_t i) { return (const void *)(req[cand[i]] + ybytes); },
-          [&](size_t i) { return (void *)(bt->d_req + i * e->slot_stride + kSlotLead + ybytes); },
+          nc, e->want - qoff, [&](size_t i) { return (const void *)(req[cand[i]] + qoff); },
+          [&](size_t i) { return (void *)(bt->d_req + i * e->slot_stride + kSlotLead + qoff); },
           cudaMemcpyHostToDevice, sc))
     return -4;
   ALTO_H(cudaEventRecord(e->ev_queries, sc));
+  if (!copy_runs(
+          nc, zbytes, [&](size_t i) { return (const void *)(req[cand[i]] + ybytes); },
+          [&](size_t i) { return (void *)(bt->d_req + i * e->slot_stride + kSlotLead + ybytes); },
+          cudaMemcpyHostToDevice, sc))
+    return -4;
+  ALTO_H(cudaEventRecord(e->ev_zkeys, sc));
 
   CUtensorMap map_q, map_y;
   if (!make_limb_maps(e, p, bt->d_qlimb, bt->d_ylimb, bp, &map_q, &map_y)) return -4;
@@ -1045,24 +1054,24 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
   if (!launch_pack(e, p, map_y, bt->d_beta, nc, st, bt->d_err)) return -4;
   ++launches;
   ALTO_H(cudaEventRecord(e->ev_pack, st));
-  // validation, the status download, the query limb split and the zeroing of the scan sums: on the side stream
-  // beside the pack once the query words are in (on the batch's stream after the pack without the overlap)
+  // the query limb split and the zeroing of the scan sums once the query words are in, then validation and the
+  // status download once the z keys are: on the side stream beside the pack (on the batch's stream after the pack
+  // without the overlap).  The scans wait for the split only; the last tail also waits for the statuses.
   cudaStream_t vs = e->overlap ? bt->side : st;
   ALTO_H(cudaStreamWaitEvent(vs, e->ev_queries, 0));
+  if (!enqueue_query_split(e, bt, bt->d_req, e->slot_stride, nc, vs)) return -4;
+  ++launches;
+  if (e->overlap) ALTO_H(cudaEventRecord(bt->ev_qready, vs));
+  ALTO_H(cudaStreamWaitEvent(vs, e->ev_zkeys, 0));
   alto::validate_kernel<<<(unsigned)nc, 256, 0, vs>>>(bt->d_req, e->slot_stride, kSlotLead, e->count, e->rows,
                                                       bt->d_status);
   ALTO_H(cudaGetLastError());
   ++launches;
   ALTO_H(cudaMemcpyAsync(bt->h_status, bt->d_status, nc * sizeof(int), cudaMemcpyDeviceToHost, vs));
   ALTO_H(cudaEventRecord(e->ev_status, vs));
-  if (!enqueue_query_split(e, bt, bt->d_req, e->slot_stride, nc, vs)) return -4;
-  ++launches;
-  if (e->overlap) {
-    ALTO_H(cudaEventRecord(bt->ev_qready, vs));
-    ALTO_H(cudaStreamWaitEvent(st, bt->ev_qready, 0));
-  }
+  if (e->overlap) ALTO_H(cudaStreamWaitEvent(st, bt->ev_qready, 0));
   if (!enqueue_scan_tails(e, bt, p, map_q, bt->d_req, e->slot_stride, nc, bt->d_resp, e->resp_len, groups,
-                          e->ev_group, &launches))
+                          e->ev_group, &launches, nullptr, e->ev_status))
     return -4;
   // the error word comes back behind the last tail, so the final synchronisation covers it
   ALTO_H(cudaMemcpyAsync(bt->h_err, bt->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
@@ -1212,6 +1221,7 @@ void *create_engine(const uint8_t *db_col, size_t ld, size_t rows, size_t cols, 
   if ((err = cudaEventCreate(&e->ev_begin)) != cudaSuccess || (err = cudaEventCreate(&e->ev_end)) != cudaSuccess ||
       (err = cudaEventCreate(&e->ev_keys)) != cudaSuccess ||
       (err = cudaEventCreateWithFlags(&e->ev_queries, cudaEventDisableTiming)) != cudaSuccess ||
+      (err = cudaEventCreateWithFlags(&e->ev_zkeys, cudaEventDisableTiming)) != cudaSuccess ||
       (err = cudaEventCreate(&e->ev_pack)) != cudaSuccess || (err = cudaEventCreate(&e->ev_status)) != cudaSuccess)
     return fail("event", err);
   for (cudaEvent_t &ev : e->ev_group)

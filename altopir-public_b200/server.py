@@ -59,7 +59,10 @@ class Server:
             self.ptr = None
 
     def __del__(self):
-        self.close()
+        # at interpreter exit the module's globals (the library handle among them) may already be gone; an
+        # explicit close() is the supported way to free device memory
+        if lib is not None:
+            self.close()
 
 
 def poisson_load(server, frames, rate_qps, seconds, seed=1, clients=4):
