@@ -115,6 +115,9 @@ def engine_local(engine):
 
     def local(slots, stride, b):
         parts = torch.zeros((b, engine.response_len()), dtype=torch.uint8, device=slots.device)
+        # the frames (the broadcast) and the zeroed parts come through torch's current stream, on which the engine's
+        # own stream does not wait
+        torch.cuda.current_stream(slots.device).synchronize()
         status = np.full(b, -1, dtype=np.int32)
         r = engine.answer_device(slots.data_ptr(), stride, b, parts.data_ptr(), engine.response_len(), status)
         if r < 0:

@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=3.0)
     ap.add_argument("--serve-clients", type=int, default=4096, help="seeded clients whose frames are replayed")
     ap.add_argument("--max-batch", type=int, default=1024)
+    ap.add_argument("--shard", action="store_true",
+                    help="column sharding: the ranks split the outputs of one engine state and answer every batch "
+                         "together (strong scaling); the default runs one whole engine per rank (replicas)")
     return ap.parse_args()
 
 
@@ -330,6 +333,7 @@ def main_ours(a):
     out_ptrs = (ctypes.c_void_p * B)(*[h_out.data_ptr() + c * rl for c in range(B)])
     h_status = np.full(B, -1, dtype=np.int32)
     stream = torch.cuda.ExternalStream(e.stream())
+    torch.cuda.synchronize()  # the buffers above were filled on torch's stream, which the engine's does not wait on
 
     peaks, peak_src = measured_peaks()
     int8_tops = int8_cublas_tops(torch) if rank == 0 else None
@@ -480,8 +484,78 @@ def main_ours(a):
     return 0
 
 
+# ------------------------------------------------------------------------------------------------ column shards
+def main_shard(a):
+    """Column sharding (altopir_b200.shard): rank r holds the columns of its output range; every step rank 0's batch
+    of frames is broadcast, each rank answers it for its parts, and the parts are all-gathered into full responses.
+    The whole job answers --batch queries per step, so `value` is strong scaling; timed on the device, max over
+    ranks.  Rank 0 checks the gathered responses against a whole engine (byte-exact)."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if "MASTER_ADDR" not in os.environ:  # one process without torchrun: a group of one
+        os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(29500 + os.getpid() % 1000))
+    dist.init_process_group("nccl", rank=rank, world_size=world, timeout=timedelta(seconds=300),
+                            device_id=torch.device("cuda", local))
+    import __graft_entry__ as ge
+    ge.load()
+    from altopir_b200 import engine as eng, service as svc, shard
+    eng.init()
+    p = svc.params(a.rows, a.record_bytes)
+    st = svc.SyntheticState.make(p, seed=1, keep_values=False)
+    ranges = shard.output_ranges(p.instances, world)
+    o0, o1 = ranges[rank]
+    e = shard.shard_engine(st, o0, o1, threads=svc.threads())
+    B, ql, part_len = a.batch, e.request_len(), st.prefixes[0].size
+    stride = (7 + ql + 255) // 256 * 256
+    slots = torch.zeros((B, stride), dtype=torch.uint8, device="cuda")
+    if rank == 0:
+        slots[:, 7:7 + ql] = torch.from_numpy(svc.synthetic_requests(p, B, seed=1000)).cuda()
+    ans = shard.ShardedAnswerer(shard.engine_local(e), ranges, part_len, "cuda")
+    for _ in range(max(3, a.warmup)):
+        status, resp = ans.answer(slots, stride, B)
+    torch.cuda.synchronize()
+    exact = None
+    if rank == 0:
+        full = eng.Engine.from_state(st, threads=svc.threads(), tile=False)
+        want = torch.zeros((B, full.response_len()), dtype=torch.uint8, device="cuda")
+        wst = np.full(B, -1, dtype=np.int32)
+        full.answer_device(slots.data_ptr(), stride, B, want.data_ptr(), full.response_len(), wst)
+        exact = bool(torch.equal(want, resp)) and list(wst) == list(status)
+        full.close()
+    dist.barrier()
+    torch.cuda.synchronize()
+    s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s_ev.record()
+    for _ in range(a.steps):
+        ans.answer(slots, stride, B)
+    e_ev.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(s_ev.elapsed_time(e_ev), world)
+    dist.barrier()
+    if rank == 0:
+        value = B * a.steps / (ms * 1e-3)  # the job's queries: every rank answers the same batch for its parts
+        cfg = config_dict(a)
+        cfg.update({"parallelism": f"columns{world}", "output_ranges": ranges,
+                    "exchange": "frames broadcast from rank 0 and parts all-gathered (NCCL) every step"})
+        print(json.dumps({"metric": METRIC, "value": value, "unit": "QPS", "n_gpus": world, "steps": a.steps,
+                          "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
+                          "scaling": "strong", "vs_baseline": None, "dtype": "u8 x u8 limbs -> int32 (exact)",
+                          "data": "synthetic", "config": cfg, "mode": "column shards",
+                          "byte_exact": {"gathered_vs_whole_engine": exact}}))
+    e.close()
+    dist.destroy_process_group()
+    return 0
+
+
 if __name__ == "__main__":
     args = parse()
     if args.serve:
         sys.exit(main_serve(args))
+    if args.shard and args.impl == "ours":
+        sys.exit(main_shard(args))
     sys.exit(main_reference(args) if args.impl == "reference" else main_ours(args))

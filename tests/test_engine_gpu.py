@@ -134,6 +134,7 @@ def test_device_resident_path_matches_host_path(gpu, svc, eng):
     slots[4, 7 + 10:7 + 13] = 0xFF
     d_out = torch.zeros((b, e.response_len()), dtype=torch.uint8, device="cuda")
     st_dev = np.full(b, -1, dtype=np.int32)
+    torch.cuda.synchronize()  # the engine's stream does not wait on torch's
     r = e.answer_device(slots.data_ptr(), stride, b, d_out.data_ptr(), e.response_len(), st_dev)
     torch.cuda.synchronize()
     assert r == b - 1 and list(st_dev) == [0, 0, 0, 0, 3, 0, 0, 0, 0]
@@ -183,6 +184,7 @@ def test_every_plan_and_the_graph_path_return_identical_bytes(gpu, svc, eng):
 
     def run():
         out = torch.zeros((b, rl), dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()  # the engine's stream does not wait on torch's
         assert e.answer_device(slots.data_ptr(), stride, b, out.data_ptr(), rl, status) == b
         return out.cpu().numpy()
 
@@ -197,6 +199,7 @@ def test_every_plan_and_the_graph_path_return_identical_bytes(gpu, svc, eng):
         assert np.array_equal(run(), want)
     for bb in (1, 5, 136):
         out = torch.zeros((bb, rl), dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()
         e.enqueue_device(slots.data_ptr(), stride, bb, out.data_ptr(), rl)
         e.sync()
         assert np.array_equal(out.cpu().numpy(), want[:bb]), bb
@@ -226,6 +229,7 @@ def test_every_schedule_returns_identical_bytes(gpu, svc, eng, monkeypatch):
         slots[:, 7:7 + ql] = torch.from_numpy(frames).cuda()
         out = torch.full((b, rl), 0x11, dtype=torch.uint8, device="cuda")
         dstat = np.full(b, -1, dtype=np.int32)
+        torch.cuda.synchronize()  # the engine's stream does not wait on torch's
         assert e.answer_device(slots.data_ptr(), stride, b, out.data_ptr(), rl, dstat) == b - 1
         assert n == b - 1 and status[3] == 3 and list(dstat) == list(status)
         dev = out.cpu().numpy()

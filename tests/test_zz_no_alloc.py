@@ -36,6 +36,7 @@ def test_noalloc_matches_answer_device_on_two_calls_in_a_row(gpu, svc, eng):
     # the existing entry point
     want = torch.full((b, rl), 0x5A, dtype=torch.uint8, device="cuda")
     want_status = np.full(b, -1, dtype=np.int32)
+    torch.cuda.synchronize()  # the engine's stream does not wait on torch's
     r = e.answer_device(slots.data_ptr(), stride, b, want.data_ptr(), rl, want_status)
     assert r == b - 1 and list(want_status) == [0, 0, 0, 3, 0, 0]
 
@@ -48,6 +49,7 @@ def test_noalloc_matches_answer_device_on_two_calls_in_a_row(gpu, svc, eng):
     for _ in range(2):
         got = torch.full((b, rl), 0x5A, dtype=torch.uint8, device="cuda")
         d_status.fill_(-1)
+        torch.cuda.synchronize()
         rc = call(got)
         assert rc == 0, pkg.last_error()
         assert torch.equal(got, want)
