@@ -112,3 +112,19 @@ def test_service_codec_roundtrip(svc):
     fr = svc.synthetic_requests(p, 3, seed=1)
     for i in range(3):
         svc.decode_request(p, fr[i])
+
+
+def test_ingest_entry_points_reject_bad_arguments_without_a_device(svc):
+    # alto_engine_new_empty checks the configuration like alto_engine_new before any CUDA call; the loaders reject a
+    # NULL engine
+    import altopir_b200 as pkg
+    L = pkg.lib()
+    dummy = np.zeros(64, dtype=np.uint8)
+    ptr = ctypes.c_void_p(dummy.ctypes.data)
+    arr = (ctypes.c_void_p * 4)(*([dummy.ctypes.data] * 4))
+    for rows, cols, n, q in ((2048, 4096, 2048, svc.Q + 2), (2048 + 32, 4096, 2048, svc.Q), (2048, 4096 + 32, 2048,
+                                                                                              svc.Q)):
+        assert not L.alto_engine_new_empty(rows, cols, ptr, n, 4, arr, 64, 0, 1024, 10, arr, ptr, q, 1)
+        assert pkg.last_error()
+    assert L.alto_engine_load_records(None, ptr, 4096, 0, 1) == -1
+    assert L.alto_engine_load_file(None, b"/nonexistent", 0) == -1
