@@ -57,8 +57,8 @@ struct PairArgs {
 };
 
 // Epilogue of 16 TMEM columns (4 clients x 4 limbs) for one accumulator row of the scan: row = database column.
-__device__ __forceinline__ void scan_epilogue16(const uint32_t (&r)[16], int col, bool row_ok, int c0, int clients,
-                                                int cols, uint32_t *out) {
+__device__ __forceinline__ void scan_epilogue16(const uint32_t *r, int col, bool row_ok, int c0, int clients, int cols,
+                                                uint32_t *out) {
 #pragma unroll
   for (int cl = 0; cl < 4; ++cl) {
     const uint32_t acc = r[4 * cl] + (r[4 * cl + 1] << 8) + (r[4 * cl + 2] << 16) + (r[4 * cl + 3] << 24);
@@ -67,23 +67,22 @@ __device__ __forceinline__ void scan_epilogue16(const uint32_t (&r)[16], int col
   }
 }
 
-// Epilogue of 16 TMEM columns for one accumulator row of the pack: row = (column, plane); the 4 planes of a column
-// are 4 adjacent lanes of one warp.
-__device__ __forceinline__ void pack_epilogue16(const uint32_t (&r)[16], int grow, bool row_ok, int c0, int clients,
+// Epilogue of 16 TMEM columns for one accumulator row of the pack: row = (column, plane j); the 4 planes of a column
+// are 4 adjacent lanes of one warp.  Each lane reduces its plane's sum S_j = sum_i G_ij 2^(8i) (< 2^57) once,
+// shifts it into place (< 2^56), and the four planes are summed in 64 bits by two shuffles (< 2^58) before the one
+// final reduction mod Q.
+__device__ __forceinline__ void pack_epilogue16(const uint32_t *r, int grow, bool row_ok, int c0, int clients,
                                                 int cols, uint32_t *out) {
   const int col = grow >> 2, plane = grow & 3;
-  const uint64_t pw = 1ull << (8 * plane);
 #pragma unroll
   for (int cl = 0; cl < 4; ++cl) {
     const uint64_t sum = (uint64_t)r[4 * cl] + ((uint64_t)r[4 * cl + 1] << 8) + ((uint64_t)r[4 * cl + 2] << 16) +
                          ((uint64_t)r[4 * cl + 3] << 24);
-    uint64_t v = mod_q64(mod_q64(sum) * pw);
-    v += __shfl_xor_sync(0xffffffffu, v, 1);
-    v = v >= kQ ? v - kQ : v;
-    v += __shfl_xor_sync(0xffffffffu, v, 2);
-    v = v >= kQ ? v - kQ : v;
+    uint64_t u = mod_q64(sum) << (8 * plane);
+    u += __shfl_xor_sync(0xffffffffu, u, 1);
+    u += __shfl_xor_sync(0xffffffffu, u, 2);
     const int c = c0 + cl;
-    if (plane == 0 && row_ok && c < clients) out[(size_t)c * cols + col] = (uint32_t)v;
+    if (plane == 0 && row_ok && c < clients) out[(size_t)c * cols + col] = (uint32_t)mod_q64(u);
   }
 }
 
@@ -244,16 +243,20 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
       const uint32_t taddr = tmem_base + (uint32_t)(ab * NSUB * BN) + ((uint32_t)(q * 32) << 16);
       const int grow = m * 256 + (int)rank * 128 + row;
       const bool row_ok = grow < args.rows_a;
+      // 32 columns per TMEM load (one wait per 8 clients instead of per 4)
 #pragma unroll 1
-      for (int ch = 0; ch < NSUB * BN / 16; ++ch) {
-        uint32_t r[16];
-        tmem_ld16(taddr + ch * 16, r);
+      for (int ch = 0; ch < NSUB * BN / 32; ++ch) {
+        uint32_t r[32];
+        tmem_ld32(taddr + ch * 32, r);
         tmem_wait_ld();
-        const int c0 = n * NSUB * (BN / 4) + ch * 4;
-        if constexpr (EPI == Epi::kScan)
-          scan_epilogue16(r, grow, row_ok, c0, args.clients, args.cols, args.out);
-        else
-          pack_epilogue16(r, grow, row_ok, c0, args.clients, args.cols, args.out);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int c0 = n * NSUB * (BN / 4) + ch * 8 + h * 4;
+          if constexpr (EPI == Epi::kScan)
+            scan_epilogue16(r + 16 * h, grow, row_ok, c0, args.clients, args.cols, args.out);
+          else
+            pack_epilogue16(r + 16 * h, grow, row_ok, c0, args.clients, args.cols, args.out);
+        }
       }
       tc_fence_before();
       __syncwarp();
