@@ -229,17 +229,21 @@ __global__ void __launch_bounds__((1 << L) / 8) tail_kernel(TailArgs a) {
     const int i0 = 8 * tid;
     const uint4 b0 = *reinterpret_cast<const uint4 *>(a.beta + base + i0);
     const uint4 b1 = *reinterpret_cast<const uint4 *>(a.beta + base + i0 + 4);
-    x[0] = b0.x; x[1] = b0.y; x[2] = b0.z; x[3] = b0.w; x[4] = b1.x; x[5] = b1.y; x[6] = b1.z; x[7] = b1.w;
+    // beta + sum_k z_k that_k, each product folded once (< 2^46) and summed in 64 bits: below 2^32 + tg 2^46 <
+    // 2^57 for every tg this engine accepts (tg n <= 32768), then reduced once
+    uint64_t acc64[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
     for (int k = 0; k < a.tg; ++k) {
       const uint4 z0 = *reinterpret_cast<const uint4 *>(z + (size_t)k * n + i0);
       const uint4 z1 = *reinterpret_cast<const uint4 *>(z + (size_t)k * n + i0 + 4);
       const uint4 t0 = *reinterpret_cast<const uint4 *>(th + (size_t)k * n + i0);
       const uint4 t1 = *reinterpret_cast<const uint4 *>(th + (size_t)k * n + i0 + 4);
-      x[0] = add_q(x[0], mul_q(z0.x, t0.x)); x[1] = add_q(x[1], mul_q(z0.y, t0.y));
-      x[2] = add_q(x[2], mul_q(z0.z, t0.z)); x[3] = add_q(x[3], mul_q(z0.w, t0.w));
-      x[4] = add_q(x[4], mul_q(z1.x, t1.x)); x[5] = add_q(x[5], mul_q(z1.y, t1.y));
-      x[6] = add_q(x[6], mul_q(z1.z, t1.z)); x[7] = add_q(x[7], mul_q(z1.w, t1.w));
+      acc64[0] += fold_q64((uint64_t)z0.x * t0.x); acc64[1] += fold_q64((uint64_t)z0.y * t0.y);
+      acc64[2] += fold_q64((uint64_t)z0.z * t0.z); acc64[3] += fold_q64((uint64_t)z0.w * t0.w);
+      acc64[4] += fold_q64((uint64_t)z1.x * t1.x); acc64[5] += fold_q64((uint64_t)z1.y * t1.y);
+      acc64[6] += fold_q64((uint64_t)z1.z * t1.z); acc64[7] += fold_q64((uint64_t)z1.w * t1.w);
     }
+#pragma unroll
+    for (int m = 0; m < 8; ++m) x[m] = red_q64(acc64[m]);
     tail_round<L>(x, tid, 0, 3, a.twiddle);
   }
 

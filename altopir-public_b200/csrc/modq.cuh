@@ -39,6 +39,9 @@ ALTO_HD uint32_t red_q64(uint64_t x) {
   return (uint32_t)(x >= kQ32 ? x - kQ32 : x);
 }
 
+// One fold of a 64-bit x: h 2^32 + l -> 12287 h + l, congruent to x mod Q and below 2^46 (not reduced).
+ALTO_HD uint64_t fold_q64(uint64_t x) { return (x >> 32) * kFold + (x & 0xffffffffull); }
+
 // (a * b) mod Q for any 32-bit a, b.
 ALTO_HD uint32_t mul_q(uint32_t a, uint32_t b) { return red_q64((uint64_t)a * b); }
 
