@@ -52,12 +52,24 @@ def test_64gib_batches_sampled_parts_match_oracle(gpu, oracle, svc, eng):
     frames = svc.synthetic_requests(p, 1024, seed=92)
     rng = np.random.default_rng(93)
     part = st.prefixes[0].size
+    first = {}
     for b in (128, 1024):
         n, status, out = _answer(e, frames, b)
         assert n == b and (status == 0).all(), b
+        first[b] = out[:64].copy()  # both batches start with the same 64 frames
         cs = rng.integers(0, b, 16)
         os_ = rng.integers(0, p.instances, 16)
         want = oracle.answer_parts(st, [frames[c] for c in cs], os_)
         for k, (c, o) in enumerate(zip(cs, os_)):
             assert np.array_equal(out[c, o * part:(o + 1) * part], want[k]), (b, c, o)
     e.close()
+    # the seeded 64-query subset, whole responses, against the reference engine itself when this host can run it
+    from oracle.oracle import RefEngine, ref_methods
+    methods = ref_methods()
+    if methods:
+        ref = RefEngine(st)
+        rr, rs, rout, _ = ref.answer([frames[c] for c in range(64)], methods[0])
+        assert rr == 64
+        for b in (128, 1024):
+            assert np.array_equal(first[b], rout), b
+        ref.close()
