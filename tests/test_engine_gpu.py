@@ -253,3 +253,21 @@ def test_record_count_off_the_tile_grid_matches_oracle(gpu, oracle, svc, eng):
     r, ost, oout = oracle.answer(st, frames_)
     assert np.array_equal(out, oout)
     e.close()
+
+
+@pytest.mark.parametrize("n,record_bytes", [(64, 4096), (256, 4096), (1024, 4096), (4096, 8192)])
+def test_other_ring_dimensions_match_oracle(gpu, oracle, svc, eng, n, record_bytes):
+    # the engine takes any power-of-two n in [16, 4096] (src/amx_kernels.cpp:551): the small-n tail, the
+    # register-blocked tail at 2^8 .. 2^12 and the GEMM tilings other than the scheme's n = 2048.  Q - 1 = 2^12 (2^20 -
+    # 3), so n = 4096 has no genuine negacyclic table; the engine and the oracle are exact for any table.
+    p = svc.Params(2048, record_bytes, n=n, tg=4)
+    st = svc.SyntheticState.make(p, seed=100 + n, full_prefix=True)
+    e = eng.Engine.from_state(st)
+    frames = svc.synthetic_requests(p, 9, seed=200 + n)
+    frames[4, 9:13] = 0xFF  # y[0] >= Q: status 3
+    n_ok, status, out = _answer(e, [frames[i] for i in range(9)], fill=0x77)
+    r, ost, oout = oracle.answer(st, [frames[i] for i in range(9)])
+    assert n_ok == r == 8 and list(status) == list(ost)
+    ok = status == 0
+    assert np.array_equal(out[ok], oout[ok]) and (out[4] == 0x77).all()
+    e.close()
