@@ -271,3 +271,23 @@ def test_other_ring_dimensions_match_oracle(gpu, oracle, svc, eng, n, record_byt
     ok = status == 0
     assert np.array_equal(out[ok], oout[ok]) and (out[4] == 0x77).all()
     e.close()
+
+
+@pytest.mark.parametrize("tg,q1_bits", [(1, 10), (2, 12), (8, 10), (4, 20)])
+def test_other_key_counts_and_row1_moduli_match_oracle(gpu, oracle, svc, eng, tg, q1_bits):
+    # tg (key blocks: the pack's K = tg n and the tail's key switch) and the row-1 modulus q1 = 2^q1_bits (the
+    # rescale and the bit packing of row 1; the engine takes q1 < 2^21), which the scheme fixes at 4 and 2^10
+    class P(svc.Params):
+        @property
+        def q1_bits(self):
+            return q1_bits
+
+    p = P(2048, 4096, tg=tg)
+    st = svc.SyntheticState.make(p, seed=300 + tg + q1_bits, full_prefix=True)
+    e = eng.Engine.from_state(st)
+    assert e.request_len() == 9 + 4 * (2 * tg * 2048 + 2048) and e.response_len() == 2 * p.part_len
+    frames = svc.synthetic_requests(p, 6, seed=400 + tg)
+    n_ok, status, out = _answer(e, [frames[i] for i in range(6)])
+    r, ost, oout = oracle.answer(st, [frames[i] for i in range(6)])
+    assert n_ok == r == 6 and np.array_equal(out, oout)
+    e.close()
