@@ -206,6 +206,7 @@ struct Batch {
     uint8_t *resp;
     bool host_status;
     cudaGraphExec_t exec;
+    int launches;  // kernels in the captured sequence (reported by alto_last_launches on every replay)
   };
   std::vector<GraphEntry> graphs;
 };
@@ -867,6 +868,7 @@ bool enqueue_batch(Engine *e, Batch *bt, const uint8_t *d_slots, size_t slot_str
     if (g.slots == slots && g.d_slots == d_slots && g.stride == slot_stride && g.resp == resp &&
         g.resp_stride == resp_stride && g.host_status == host_status) {
       ALTO_CK(cudaGraphLaunch(g.exec, bt->st));
+      e->last_launches = g.launches;
       return true;
     }
   ALTO_CK(cudaStreamBeginCapture(bt->st, cudaStreamCaptureModeThreadLocal));
@@ -887,7 +889,7 @@ bool enqueue_batch(Engine *e, Batch *bt, const uint8_t *d_slots, size_t slot_str
     cudaGraphExecDestroy(bt->graphs.front().exec);
     bt->graphs.erase(bt->graphs.begin());
   }
-  bt->graphs.push_back({slots, slot_stride, resp_stride, d_slots, resp, host_status, exec});
+  bt->graphs.push_back({slots, slot_stride, resp_stride, d_slots, resp, host_status, exec, e->last_launches});
   ALTO_CK(cudaGraphLaunch(exec, bt->st));
   return true;
 }

@@ -197,6 +197,7 @@ def test_every_plan_and_the_graph_path_return_identical_bytes(gpu, svc, eng):
     e.set_graphs(True)
     for _ in range(3):  # capture on the first call, replay after
         assert np.array_equal(run(), want)
+        assert e.last_launches() > 0  # a replay reports the kernels of its captured sequence
     for bb in (1, 5, 136):
         out = torch.zeros((bb, rl), dtype=torch.uint8, device="cuda")
         torch.cuda.synchronize()
