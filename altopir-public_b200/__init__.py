@@ -50,6 +50,10 @@ def _declare(L):
         "alto_engine_set_graphs": (I, [P, I]),
         "alto_engine_set_tuning": (I, [P, P, S]),
         "alto_answer_device_noalloc": (I, [P, P, S, S, P, S, P]),
+        "alto_answer_device_parts": (I, [P, P, S, S, PP, S, S, S, c.POINTER(I)]),
+        "alto_ipc_export": (I, [P, P]),
+        "alto_ipc_import": (P, [P]),
+        "alto_ipc_release": (I, [P]),
         "alto_server_new": (P, [P, S, S, I]),
         "alto_server_new_loopback": (P, [S, S, S, S, I, c.c_double]),
         "alto_server_submit": (c.c_longlong, [P, P, S]),
@@ -83,7 +87,9 @@ EXPORTS = (
     "sw_amx_init", "sw_alloc_zeroed", "sw_alloc", "sw_free", "sw_tile_db", "sw_pack_build", "alto_engine_new",
     "alto_engine_free", "alto_request_len", "alto_response_len", "alto_answer", "alto_last_error",
     "alto_answer_device", "alto_last_launches", "alto_enqueue_device", "alto_engine_sync", "alto_engine_stream",
-    "alto_kernel_times", "alto_engine_set_graphs", "alto_engine_set_tuning", "alto_answer_device_noalloc", "alto_server_new", "alto_server_new_loopback",
+    "alto_kernel_times", "alto_engine_set_graphs", "alto_engine_set_tuning", "alto_answer_device_noalloc",
+    "alto_answer_device_parts", "alto_ipc_export", "alto_ipc_import", "alto_ipc_release", "alto_server_new",
+    "alto_server_new_loopback",
     "alto_server_submit", "alto_server_wait", "alto_server_stats", "alto_server_free", "alto_engine_new_empty",
     "alto_engine_load_records", "alto_engine_load_file", "alto_synthetic_db_col", "alto_synthetic_db_col_device",
     "alto_fill_uniform_u32", "alto_fill_uniform_u64", "alto_fill_bytes", "alto_synthetic_request",

@@ -40,6 +40,7 @@ void set_error(const std::string &msg) { g_last_error = msg; }
 constexpr size_t kSlotLead = 7;  // frame offset inside a staging slot: puts the key words on a 16-byte boundary
 constexpr int kMarks = 7;          // timing marks per batch (see enqueue_batch)
 constexpr int kTimingSets = 128;   // batches that may be in flight with timing marks
+constexpr size_t kMaxGather = 64;  // response buffers one alto_answer_device_parts call may write into
 
 // ------------------------------------------------------------------------------------------- tensor maps
 using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -199,6 +200,10 @@ struct Batch {
   // but the last beside the scan of the next group.  It forks from and joins back into `st` inside every batch.
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_qready = nullptr, ev_join = nullptr, ev_scan[8] = {};
+  // alto_answer_device_parts: the response buffers the tails write every part into (device array of pointers,
+  // allocated on first use), their count for the batch being enqueued (0 otherwise) and this engine's first part
+  uint8_t **d_gather = nullptr;
+  int n_gather = 0, gather_offset = 0;
   // CUDA graphs of the device-side launch sequence, one per batch size and buffer set (see enqueue_batch)
   struct GraphEntry {
     size_t slots, stride, resp_stride;
@@ -375,6 +380,8 @@ void destroy_batch(Batch *b) {
   if (b->st) cudaStreamSynchronize(b->st);
   if (b->side) cudaStreamSynchronize(b->side);
   free_scratch(b);
+  cudaFree(b->d_gather);
+  b->d_gather = nullptr;
   cudaFree(b->d_err);
   cudaFreeHost(b->h_err);
   for (cudaEvent_t ev : {b->ev_fork, b->ev_qready, b->ev_join})
@@ -734,6 +741,9 @@ alto::TailArgs tail_args(const Engine *e, const Batch *bt, const uint8_t *d_slot
   t.q1 = (int64_t)e->q1;
   t.o_begin = o_begin;
   t.o_count = o_count;
+  t.resp_list = bt->n_gather ? bt->d_gather : nullptr;
+  t.n_resp = bt->n_gather;
+  t.part_offset = bt->gather_offset;
   return t;
 }
 
@@ -1385,6 +1395,85 @@ int alto_answer_device(void *p, const uint8_t *d_req, size_t req_stride, size_t 
     valid += status[c] == 0;
   }
   return valid;
+}
+
+int alto_answer_device_parts(void *p, const uint8_t *d_req, size_t req_stride, size_t b, uint8_t *const *d_outs,
+                             size_t n_outs, size_t out_stride, size_t part_offset, int *status) {
+  Engine *e = static_cast<Engine *>(p);
+  if (!e || !d_req || !d_outs || !status || !n_outs || n_outs > kMaxGather || req_stride % 16 ||
+      req_stride < round_up(kSlotLead + e->want, 16) || out_stride < (part_offset + e->outputs) * e->part_len) {
+    set_error("alto_answer_device_parts: bad arguments");
+    return -1;
+  }
+  for (size_t k = 0; k < n_outs; ++k)
+    if (!d_outs[k]) {
+      set_error("alto_answer_device_parts: NULL output buffer");
+      return -1;
+    }
+  e->last_launches = 0;
+  if (!b) return 0;
+  if (!e->tail_ok) return -3;
+  Batch *bt = &e->main;
+  if (cudaSetDevice(e->dev) != cudaSuccess || !ensure_capacity(e, bt, b)) return -4;
+  if (!bt->d_gather && cudaMalloc(&bt->d_gather, kMaxGather * sizeof(uint8_t *)) != cudaSuccess) {
+    set_error("gather list", cudaGetLastError());
+    return -4;
+  }
+  // the previous batch may still read the list; the copy from the caller's array must finish before it returns
+  if (cudaStreamSynchronize(bt->st) != cudaSuccess ||
+      cudaMemcpy(bt->d_gather, d_outs, n_outs * sizeof(uint8_t *), cudaMemcpyHostToDevice) != cudaSuccess) {
+    set_error("gather list", cudaGetLastError());
+    return -4;
+  }
+  bt->n_gather = (int)n_outs;
+  bt->gather_offset = (int)part_offset;
+  // launched directly: a captured graph would hold this call's destinations
+  const bool ok = enqueue_batch_direct(e, bt, d_req, req_stride, b, nullptr, out_stride, true, true);
+  bt->n_gather = 0;
+  bt->gather_offset = 0;
+  if (!ok || !finish(e, nullptr)) return -4;
+  int valid = 0;
+  for (size_t c = 0; c < b; ++c) {
+    status[c] = bt->h_status[c];
+    valid += status[c] == 0;
+  }
+  return valid;
+}
+
+int alto_ipc_export(const void *d_ptr, uint8_t *handle) {
+  if (!d_ptr || !handle) return -1;
+  cudaIpcMemHandle_t h;
+  const cudaError_t err = cudaIpcGetMemHandle(&h, const_cast<void *>(d_ptr));
+  if (err != cudaSuccess) {
+    set_error("cudaIpcGetMemHandle", err);
+    return -4;
+  }
+  static_assert(sizeof(h) == 64, "CUDA IPC handles are 64 bytes");
+  memcpy(handle, &h, sizeof(h));
+  return 0;
+}
+
+void *alto_ipc_import(const uint8_t *handle) {
+  if (!handle) return nullptr;
+  cudaIpcMemHandle_t h;
+  memcpy(&h, handle, sizeof(h));
+  void *p = nullptr;
+  const cudaError_t err = cudaIpcOpenMemHandle(&p, h, cudaIpcMemLazyEnablePeerAccess);
+  if (err != cudaSuccess) {
+    set_error("cudaIpcOpenMemHandle", err);
+    return nullptr;
+  }
+  return p;
+}
+
+int alto_ipc_release(void *d_ptr) {
+  if (!d_ptr) return -1;
+  const cudaError_t err = cudaIpcCloseMemHandle(d_ptr);
+  if (err != cudaSuccess) {
+    set_error("cudaIpcCloseMemHandle", err);
+    return -4;
+  }
+  return 0;
 }
 
 int alto_enqueue_device(void *p, const uint8_t *d_req, size_t req_stride, size_t b, uint8_t *d_out, size_t out_stride,

@@ -156,7 +156,19 @@ struct TailArgs {
   int part_len, row1_off, q1_bits;
   int64_t q1;
   int o_begin, o_count;     // this launch answers parts o_begin .. o_begin + o_count of every slot
+  // Gather into several response buffers (column shards): when n_resp > 0 the part is written to every
+  // resp_list[k] + s * resp_stride + (part_offset + o) * part_len instead of to resp -- buffers of this GPU or of
+  // peer GPUs (CUDA IPC mappings over NVLink), so the shards' all-gather happens in this kernel's stores.
+  uint8_t *const *resp_list = nullptr;
+  int n_resp = 0;
+  int part_offset = 0;
 };
+
+// The destinations of response part o of slot `slot`: resp, or each gather buffer (see TailArgs).
+__device__ __forceinline__ uint8_t *tail_dst(const TailArgs &a, int k, int slot, int o) {
+  uint8_t *base = a.n_resp ? a.resp_list[k] : a.resp;
+  return base + (size_t)slot * a.resp_stride + (size_t)(a.part_offset + o) * a.part_len;
+}
 
 // One response part per CTA (slot, output o), n / 8 threads owning 8 coefficients each.
 //   acc[i] = beta[i] + sum_k z[k n + i] * that[k n + i] (mod Q)                    (src/amx_kernels.cpp:500-511)
@@ -291,12 +303,15 @@ __global__ void __launch_bounds__((1 << L) / 8) tail_kernel(TailArgs a) {
   }
   __syncthreads();
 
-  uint8_t *dst = a.resp + (size_t)slot * a.resp_stride + (size_t)o * a.part_len;
-  if ((a.part_len & 15) == 0 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
-    for (int w = tid; w < a.part_len / 16; w += NT)
-      *reinterpret_cast<uint4 *>(dst + 16 * w) = make_uint4(res[4 * w], res[4 * w + 1], res[4 * w + 2], res[4 * w + 3]);
-  } else {
-    for (int b = tid; b < a.part_len; b += NT) dst[b] = (uint8_t)(res[b >> 2] >> (8 * (b & 3)));
+  for (int k = 0; k < (a.n_resp ? a.n_resp : 1); ++k) {
+    uint8_t *dst = tail_dst(a, k, slot, o);
+    if ((a.part_len & 15) == 0 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+      for (int w = tid; w < a.part_len / 16; w += NT)
+        *reinterpret_cast<uint4 *>(dst + 16 * w) =
+            make_uint4(res[4 * w], res[4 * w + 1], res[4 * w + 2], res[4 * w + 3]);
+    } else {
+      for (int b = tid; b < a.part_len; b += NT) dst[b] = (uint8_t)(res[b >> 2] >> (8 * (b & 3)));
+    }
   }
 }
 
@@ -349,8 +364,10 @@ __global__ void __launch_bounds__(128) tail_small_kernel(TailArgs a) {
     }
   }
   __syncthreads();
-  uint8_t *dst = a.resp + (size_t)slot * a.resp_stride + (size_t)o * a.part_len;
-  for (int b = tid; b < a.part_len; b += nt) dst[b] = (uint8_t)(res[b >> 2] >> (8 * (b & 3)));
+  for (int k = 0; k < (a.n_resp ? a.n_resp : 1); ++k) {
+    uint8_t *dst = tail_dst(a, k, slot, o);
+    for (int b = tid; b < a.part_len; b += nt) dst[b] = (uint8_t)(res[b >> 2] >> (8 * (b & 3)));
+  }
 }
 
 // ------------------------------------------------------------------------------------ synthetic database

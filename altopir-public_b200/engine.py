@@ -159,6 +159,14 @@ class Engine:
         return lib().alto_answer_device(self.ptr, ctypes.c_void_p(d_req), req_stride, b, ctypes.c_void_p(d_out),
                                         out_stride, status.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), stage)
 
+    def answer_device_parts(self, d_req, req_stride, b, d_outs, out_stride, part_offset, status):
+        """alto_answer_device_parts: this shard's response parts written into every buffer of d_outs (device
+        pointers, local or mapped from other GPUs) at column offset part_offset * part_len."""
+        outs = (ctypes.c_void_p * len(d_outs))(*d_outs)
+        return lib().alto_answer_device_parts(self.ptr, ctypes.c_void_p(d_req), req_stride, b, outs, len(d_outs),
+                                              out_stride, part_offset,
+                                              status.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+
     def enqueue_device(self, d_req, req_stride, b, d_out, out_stride, d_status=None):
         """alto_enqueue_device: enqueue without waiting; check completion with sync()."""
         r = lib().alto_enqueue_device(self.ptr, ctypes.c_void_p(d_req), req_stride, b, ctypes.c_void_p(d_out),

@@ -125,3 +125,67 @@ def engine_local(engine):
         return status, parts
 
     return local
+
+
+class PeerGather:
+    """Column shards whose tails do the all-gather: every rank's tail kernel writes its response parts straight into
+    every rank's full-width response buffer -- its own, and the other ranks' through CUDA IPC mappings (NVLink
+    stores between GPUs) -- so that after each call and one barrier every rank holds the full responses, and no
+    collective moves response bytes (alto_answer_device_parts).
+
+    `engine` is this rank's shard engine over outputs ranges[rank]; `buffer` is this rank's (b_max, full width)
+    device tensor of responses, overwritten by every call.  The IPC handles are exchanged once, here, with
+    all_gather_object over the process group (any backend).  Call close() on every rank before the group ends."""
+
+    def __init__(self, engine, ranges, part_len, b_max, group=None):
+        import ctypes
+        import torch
+        import torch.distributed as dist
+        from . import lib, last_error
+        self.dist, self.group, self.engine = dist, group, engine
+        self.rank, self.world = dist.get_rank(group), dist.get_world_size(group)
+        assert len(ranges) == self.world
+        self.offset = ranges[self.rank][0]
+        self.buffer = torch.zeros((b_max, ranges[-1][1] * part_len), dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()
+        h = (ctypes.c_uint8 * 64)()
+        if lib().alto_ipc_export(self.buffer.data_ptr(), h) != 0:
+            raise RuntimeError(f"alto_ipc_export: {last_error()}")
+        handles = [None] * self.world
+        dist.all_gather_object(handles, bytes(h), group=group)
+        self.mapped, self.dsts = [], []
+        for r, hb in enumerate(handles):
+            if r == self.rank:
+                self.dsts.append(self.buffer.data_ptr())
+                continue
+            p = lib().alto_ipc_import((ctypes.c_uint8 * 64).from_buffer_copy(hb))
+            if not p:
+                raise RuntimeError(f"alto_ipc_import of rank {r}: {last_error()}")
+            self.mapped.append(p)
+            self.dsts.append(p)
+
+    def answer(self, slots, stride, b, src=None):
+        """Answers frames resident in device memory (frame c at slots + c * stride + 7), the same frames on every
+        rank (broadcast from rank `src` first when given).  Returns (statuses, this rank's full responses, rows
+        :b), complete on every rank when the call returns on any and valid until the next call (which first waits
+        for every rank to arrive, so no rank overwrites responses another is still reading)."""
+        import torch
+        self.dist.barrier(group=self.group)  # every rank is done with the previous call's responses
+        if src is not None:
+            self.dist.broadcast(slots, src=src, group=self.group)
+        torch.cuda.current_stream().synchronize()  # the engine's stream does not wait on torch's
+        status = np.full(b, -1, dtype=np.int32)
+        r = self.engine.answer_device_parts(slots.data_ptr(), stride, b, self.dsts, self.buffer.shape[1],
+                                            self.offset, status)
+        if r < 0:
+            from . import last_error
+            raise RuntimeError(f"engine error {r}: {last_error()}")
+        self.dist.barrier(group=self.group)  # every shard's parts are in every buffer
+        return status, self.buffer[:b]
+
+    def close(self):
+        from . import lib
+        self.dist.barrier(group=self.group)  # no rank writes into a mapping after this
+        for p in self.mapped:
+            lib().alto_ipc_release(p)
+        self.mapped = []

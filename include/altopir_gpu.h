@@ -98,6 +98,23 @@ const char *alto_last_error(void);
 int alto_answer_device(void *engine, const uint8_t *d_req, size_t req_stride, size_t b, uint8_t *d_out,
                        size_t out_stride, int *status, double *stage_ms);
 
+/* Column shards (a database split by output ranges over several GPUs, one engine per GPU over its columns):
+ * alto_answer_device for an engine that holds outputs [part_offset, part_offset + its outputs) of the full response,
+ * writing every valid frame's parts into each buffer d_outs[k], at d_outs[k] + c * out_stride +
+ * (part_offset + o) * part_len.  The buffers may be this GPU's or other GPUs' (mapped with alto_ipc_import): once
+ * every shard has answered the same frames, each buffer holds the full responses -- the shards' all-gather is done
+ * by the tail kernel's own stores, over NVLink between GPUs, with no separate collective.  1 <= n_outs <= 64,
+ * out_stride >= (part_offset + outputs) * part_len; statuses to the host array status[b].  Returns the number of
+ * valid frames, or -1/-3/-4 as alto_answer_device.  The caller orders the shards' calls with the readers of the
+ * buffers (a barrier between ranks after every call).
+ * alto_ipc_export writes the 64-byte CUDA IPC handle of a device allocation into handle[64] (0, -1, -4);
+ * alto_ipc_import maps another process's handle into this one (NULL on failure); alto_ipc_release unmaps it. */
+int alto_answer_device_parts(void *engine, const uint8_t *d_req, size_t req_stride, size_t b, uint8_t *const *d_outs,
+                             size_t n_outs, size_t out_stride, size_t part_offset, int *status);
+int alto_ipc_export(const void *d_ptr, uint8_t *handle);
+void *alto_ipc_import(const uint8_t *handle);
+int alto_ipc_release(void *d_ptr);
+
 /* Count of kernel launches issued by the most recent batch of this engine. */
 int alto_last_launches(const void *engine);
 
