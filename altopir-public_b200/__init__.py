@@ -51,7 +51,7 @@ def _declare(L):
         "alto_engine_set_tuning": (I, [P, P, S]),
         "alto_answer_device_noalloc": (I, [P, P, S, S, P, S, P]),
         "alto_answer_device_parts": (I, [P, P, S, S, PP, S, S, S, c.POINTER(I)]),
-        "alto_ipc_export": (I, [P, P]),
+        "alto_ipc_export": (I, [P, P, c.POINTER(S)]),
         "alto_ipc_import": (P, [P]),
         "alto_ipc_release": (I, [P]),
         "alto_server_new": (P, [P, S, S, I]),

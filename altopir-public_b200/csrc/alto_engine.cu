@@ -1440,16 +1440,34 @@ int alto_answer_device_parts(void *p, const uint8_t *d_req, size_t req_stride, s
   return valid;
 }
 
-int alto_ipc_export(const void *d_ptr, uint8_t *handle) {
-  if (!d_ptr || !handle) return -1;
+int alto_ipc_export(const void *d_ptr, uint8_t *handle, size_t *offset) {
+  if (!d_ptr || !handle || !offset) return -1;
+  // An IPC handle names a whole allocation and opens at its base; d_ptr may lie inside a larger one (a caching
+  // allocator's segment), so the handle is taken for the base and the offset travels with it.
+  using AddressRangeFn = CUresult (*)(CUdeviceptr *, size_t *, CUdeviceptr);
+  static AddressRangeFn range_fn = nullptr;
+  if (!range_fn) {
+    void *fp = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &fp, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      range_fn = reinterpret_cast<AddressRangeFn>(fp);
+  }
+  CUdeviceptr base = 0;
+  size_t size = 0;
+  if (!range_fn || range_fn(&base, &size, reinterpret_cast<CUdeviceptr>(d_ptr)) != CUDA_SUCCESS) {
+    set_error("cuMemGetAddressRange failed: not a device allocation of this process");
+    return -4;
+  }
   cudaIpcMemHandle_t h;
-  const cudaError_t err = cudaIpcGetMemHandle(&h, const_cast<void *>(d_ptr));
+  const cudaError_t err = cudaIpcGetMemHandle(&h, reinterpret_cast<void *>(base));
   if (err != cudaSuccess) {
     set_error("cudaIpcGetMemHandle", err);
     return -4;
   }
   static_assert(sizeof(h) == 64, "CUDA IPC handles are 64 bytes");
   memcpy(handle, &h, sizeof(h));
+  *offset = reinterpret_cast<CUdeviceptr>(d_ptr) - base;
   return 0;
 }
 

@@ -148,21 +148,24 @@ class PeerGather:
         self.offset = ranges[self.rank][0]
         self.buffer = torch.zeros((b_max, ranges[-1][1] * part_len), dtype=torch.uint8, device="cuda")
         torch.cuda.synchronize()
-        h = (ctypes.c_uint8 * 64)()
-        if lib().alto_ipc_export(self.buffer.data_ptr(), h) != 0:
+        # the buffer may sit inside a larger allocation of torch's caching allocator: the handle names that
+        # allocation, and the buffer's offset in it travels with the handle
+        h, off = (ctypes.c_uint8 * 64)(), ctypes.c_size_t(0)
+        if lib().alto_ipc_export(self.buffer.data_ptr(), h, ctypes.byref(off)) != 0:
             raise RuntimeError(f"alto_ipc_export: {last_error()}")
         handles = [None] * self.world
-        dist.all_gather_object(handles, bytes(h), group=group)
+        self.export_offset = off.value
+        dist.all_gather_object(handles, (bytes(h), off.value), group=group)
         self.mapped, self.dsts = [], []
-        for r, hb in enumerate(handles):
+        for r, (hb, offset) in enumerate(handles):
             if r == self.rank:
                 self.dsts.append(self.buffer.data_ptr())
                 continue
-            p = lib().alto_ipc_import((ctypes.c_uint8 * 64).from_buffer_copy(hb))
-            if not p:
+            base = lib().alto_ipc_import((ctypes.c_uint8 * 64).from_buffer_copy(hb))
+            if not base:
                 raise RuntimeError(f"alto_ipc_import of rank {r}: {last_error()}")
-            self.mapped.append(p)
-            self.dsts.append(p)
+            self.mapped.append(base)
+            self.dsts.append(base + offset)
 
     def answer(self, slots, stride, b, src=None):
         """Answers frames resident in device memory (frame c at slots + c * stride + 7), the same frames on every

@@ -107,11 +107,13 @@ int alto_answer_device(void *engine, const uint8_t *d_req, size_t req_stride, si
  * out_stride >= (part_offset + outputs) * part_len; statuses to the host array status[b].  Returns the number of
  * valid frames, or -1/-3/-4 as alto_answer_device.  The caller orders the shards' calls with the readers of the
  * buffers (a barrier between ranks after every call).
- * alto_ipc_export writes the 64-byte CUDA IPC handle of a device allocation into handle[64] (0, -1, -4);
- * alto_ipc_import maps another process's handle into this one (NULL on failure); alto_ipc_release unmaps it. */
+ * alto_ipc_export writes the 64-byte CUDA IPC handle of the device allocation that contains d_ptr into handle[64]
+ * and d_ptr's offset inside it into *offset (0, -1, -4); alto_ipc_import maps another process's handle into this
+ * one and returns the base of the mapping (NULL on failure) -- the exporter's pointer is that base plus the offset;
+ * alto_ipc_release unmaps a base returned by alto_ipc_import. */
 int alto_answer_device_parts(void *engine, const uint8_t *d_req, size_t req_stride, size_t b, uint8_t *const *d_outs,
                              size_t n_outs, size_t out_stride, size_t part_offset, int *status);
-int alto_ipc_export(const void *d_ptr, uint8_t *handle);
+int alto_ipc_export(const void *d_ptr, uint8_t *handle, size_t *offset);
 void *alto_ipc_import(const uint8_t *handle);
 int alto_ipc_release(void *d_ptr);
 

@@ -42,8 +42,12 @@ def _rank(rank, world, port, out):
     e = shard.shard_engine(st, *ranges[rank])
     ql, part = svc.request_len(p), st.prefixes[0].size
     stride = (7 + ql + 15) // 16 * 16
+    # a small tensor first, so that the gather buffer sits inside the same caching-allocator segment at an offset:
+    # the IPC handle names the segment, and the offset must travel with it
+    pad = torch.zeros(1024, dtype=torch.uint8, device="cuda")
     gather = shard.PeerGather(e, ranges, part, b_max=8)
-    ok = True
+    ok = gather.export_offset > 0
+    del pad
     for call in range(2):  # two calls in a row over the same buffers
         b = 6 if call == 0 else 8
         frames = svc.synthetic_requests(p, b, seed=112 + call)
