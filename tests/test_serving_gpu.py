@@ -6,6 +6,9 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
+# the loop's host waits are bounded (60 s a ticket); the whole test is bounded too, so that a stalled loop fails
+# the run instead of holding it
+@pytest.mark.timeout(300, method="thread")
 def test_each_result_is_the_same_alone_and_in_the_mix(gpu, svc, eng):
     from altopir_b200 import server as srv
     import frames as fr
