@@ -317,11 +317,13 @@ int alto_server_wait(void *p, long long id, uint8_t *out, size_t out_len, int ti
   std::unique_lock<std::mutex> lk(s->mu);
   auto it = s->tickets.find(id);
   if (it == s->tickets.end()) return -1;
-  if (!s->cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return it->second.done; })) return -5;
-  const int st = it->second.status;
-  if (st == 0 && out) memcpy(out, it->second.resp.data(), std::min(out_len, s->resp_len));
-  if (latency_ms) *latency_ms = 1e3 * (it->second.t_done - it->second.t_submit);
-  s->tickets.erase(it);
+  // submitters insert tickets while this thread waits, and a rehash invalidates iterators but not references
+  const Ticket &t = it->second;
+  if (!s->cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return t.done; })) return -5;
+  const int st = t.status;
+  if (st == 0 && out) memcpy(out, t.resp.data(), std::min(out_len, s->resp_len));
+  if (latency_ms) *latency_ms = 1e3 * (t.t_done - t.t_submit);
+  s->tickets.erase(id);
   return st;
 }
 
