@@ -259,8 +259,12 @@ struct Engine {
   bool use_graphs = false;  // replay captured launch sequences (alto_engine_set_graphs)
   bool overlap = true;      // the two-stream schedule of a batch (ALTO_OVERLAP=0 runs it on one stream)
   int groups = 2;           // column groups of the scan and tail of a device batch (ALTO_GROUPS: 1, 2, 4 or 8)
-  int host_groups = 4;      // the same for alto_answer, whose groups' downloads overlap (ALTO_HOST_GROUPS); its
-                            // last group is half the size of the others (less left to download after the last scan)
+  // The column groups of alto_answer, whose downloads overlap the scan, as weights (ALTO_HOST_WEIGHTS, or
+  // ALTO_HOST_GROUPS groups with a last one of half the size).  A group's tail runs once the next group's scan has
+  // left the SMs, so the last two groups' tails and downloads follow the last scan.  At 1 GiB and B = 128, 2,2,2,1
+  // (5, 4, 5 and 2 of 16 parts) measured fastest with 6,4,3,2,1 (1.10 ms a call); 6,5,3,2, 5,5,4,2, 8,4,4, 8,4,2,2,
+  // 8,4,2,1,1 and 7,5,3,1 took 1.11-1.14 ms: what they save after the last scan, their smaller groups' scans cost.
+  std::vector<int> host_weights = {2, 2, 2, 1};
   std::vector<TuneEntry> tuning;  // sorted by b_max; the first entry with b_max >= batch size applies
 };
 
@@ -691,29 +695,46 @@ struct Groups {
   int tiles_per_part = 0;
 };
 
-// `want` groups of (nearly) equal size, or with `small_last` a last group of half the size of the others, so that
-// less of the work -- its tail and, in alto_answer, its download -- is left once the last scan ends.
-Groups column_groups(const Engine *e, const Plan &p, int want, bool small_last = false) {
+// Column groups whose sizes follow `weights` (the first 8 count, each > 0): group i ends at part
+// round(outputs * (w_0 + ... + w_i) / total), the last at `outputs`; empty groups are dropped.
+Groups column_groups(const Engine *e, const Plan &p, const std::vector<int> &weights) {
   Groups g;
   const int tile_cols = p.pair ? 256 : 128;
   g.bounds[1] = (int)e->outputs;
-  if (want <= 1 || e->n % tile_cols) return g;
+  const int count = std::min<int>((int)weights.size(), 8);
+  if (count <= 1 || e->n % tile_cols) return g;
   g.tiles_per_part = (int)(e->n / tile_cols);
-  const int count = std::min<int>(std::min(want, 8), (int)e->outputs);
-  // weights: 2 for every group, 1 for a small last one
-  const int total = 2 * count - (small_last ? 1 : 0);
-  int acc = 0;
-  for (int i = 0; i < count; ++i) {
-    acc += (small_last && i + 1 == count) ? 1 : 2;
-    g.bounds[i + 1] = (int)((e->outputs * (size_t)acc + total / 2) / total);
-  }
-  g.bounds[count] = (int)e->outputs;
-  // drop empty groups
+  long total = 0, acc = 0;
+  for (int i = 0; i < count; ++i) total += weights[i];
   int k = 0;
-  for (int i = 1; i <= count; ++i)
-    if (g.bounds[i] > g.bounds[k]) g.bounds[++k] = g.bounds[i];
+  for (int i = 0; i < count; ++i) {
+    acc += weights[i];
+    const int b = i + 1 == count ? (int)e->outputs : (int)(((long)e->outputs * acc + total / 2) / total);
+    if (b > g.bounds[k]) g.bounds[++k] = b;
+  }
   g.count = k;
   return g;
+}
+
+// Weights of `count` equal groups, or of equal groups but a last one of half the size.
+std::vector<int> group_weights(int count, bool small_last) {
+  std::vector<int> w(std::max(1, std::min(count, 8)), 2);
+  if (small_last && w.size() > 1) w.back() = 1;
+  return w;
+}
+
+// A comma-separated list of 1 to 8 positive weights; empty when malformed.
+std::vector<int> parse_weights(const char *v) {
+  std::vector<int> w;
+  const char *s = v;
+  while (*s) {
+    char *end = nullptr;
+    const long x = strtol(s, &end, 10);
+    if (end == s || x <= 0 || x > 1024 || w.size() == 8 || (*end && *end != ',')) return {};
+    w.push_back((int)x);
+    s = *end ? end + 1 : end;
+  }
+  return w;
 }
 
 // Tail arguments for the output parts [o_begin, o_begin + o_count) of every frame.
@@ -804,7 +825,7 @@ bool enqueue_batch_direct(Engine *e, Batch *bt, const uint8_t *d_slots, size_t s
                           uint8_t *resp, size_t resp_stride, bool host_status, bool with_marks) {
   cudaStream_t st = bt->st;
   const Plan p = make_plan(e, slots);
-  const Groups groups = column_groups(e, p, e->overlap ? e->groups : 1);
+  const Groups groups = column_groups(e, p, group_weights(e->overlap ? e->groups : 1, false));
   const int bp = (int)round_up(slots, 4);
   int launches = 0;
   // timing marks (main batch only): 0 begin | validate (one stream only) | 1 | y split | 2 | pack | 3 | (wait for
@@ -1020,7 +1041,7 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
   cudaStream_t st = bt->st, sc = e->st_copy;
   const size_t nc = cand.size();
   const Plan p = make_plan(e, nc);
-  const Groups groups = column_groups(e, p, e->overlap ? e->host_groups : 1, true);
+  const Groups groups = column_groups(e, p, e->overlap ? e->host_weights : std::vector<int>{1});
   const int bp = (int)round_up(nc, 4);
   const size_t ybytes = 9 + 4 * e->count;  // header and y keys
   int launches = 0;
@@ -1229,7 +1250,11 @@ void *create_engine(const uint8_t *db_col, size_t ld, size_t rows, size_t cols, 
   if ((err = cudaStreamCreateWithFlags(&e->st_copy, cudaStreamNonBlocking)) != cudaSuccess) return fail("stream", err);
   if (const char *v = getenv("ALTO_OVERLAP")) e->overlap = v[0] != '0';
   if (const char *v = getenv("ALTO_GROUPS")) e->groups = std::max(1, std::min(8, atoi(v)));
-  if (const char *v = getenv("ALTO_HOST_GROUPS")) e->host_groups = std::max(1, std::min(8, atoi(v)));
+  if (const char *v = getenv("ALTO_HOST_GROUPS")) e->host_weights = group_weights(atoi(v), true);
+  if (const char *v = getenv("ALTO_HOST_WEIGHTS")) {
+    std::vector<int> w = parse_weights(v);
+    if (!w.empty()) e->host_weights = w;
+  }
   if ((err = cudaEventCreate(&e->ev_begin)) != cudaSuccess || (err = cudaEventCreate(&e->ev_end)) != cudaSuccess ||
       (err = cudaEventCreate(&e->ev_keys)) != cudaSuccess ||
       (err = cudaEventCreateWithFlags(&e->ev_queries, cudaEventDisableTiming)) != cudaSuccess ||

@@ -210,7 +210,8 @@ def test_every_plan_and_the_graph_path_return_identical_bytes(gpu, svc, eng):
 
 def test_every_schedule_returns_identical_bytes(gpu, svc, eng, monkeypatch):
     # one stream or two (ALTO_OVERLAP), and 1..8 column groups for the device path (ALTO_GROUPS) and alto_answer
-    # (ALTO_HOST_GROUPS); the knobs are read when an engine is created
+    # (ALTO_HOST_GROUPS, or group sizes as weights in ALTO_HOST_WEIGHTS, which wins; a malformed list is ignored);
+    # the knobs are read when an engine is created
     import torch
     p = svc.params(4096, 32768)  # 16 response parts, so every group count divides
     st = svc.SyntheticState.make(p, seed=41)
@@ -218,10 +219,17 @@ def test_every_schedule_returns_identical_bytes(gpu, svc, eng, monkeypatch):
     frames = svc.synthetic_requests(p, b, seed=42)
     frames[3, 9:13] = 0xFF  # y[0] >= Q: status 3
     want = None
-    for overlap, groups, host_groups in ((0, 1, 1), (1, 1, 1), (1, 2, 2), (1, 4, 4), (1, 8, 8), (1, 2, 4)):
+    for overlap, groups, host_groups, weights in ((0, 1, 1, None), (1, 1, 1, None), (1, 2, 2, None), (1, 4, 4, None),
+                                                  (1, 8, 8, None), (1, 2, 4, None), (1, 2, 4, "8,4,2,1,1"),
+                                                  (1, 2, 4, "6,5,3,2"), (1, 2, 4, "1,1,1,1,1,1,1,1"),
+                                                  (1, 2, 3, "3,x")):
         monkeypatch.setenv("ALTO_OVERLAP", str(overlap))
         monkeypatch.setenv("ALTO_GROUPS", str(groups))
         monkeypatch.setenv("ALTO_HOST_GROUPS", str(host_groups))
+        if weights is None:
+            monkeypatch.delenv("ALTO_HOST_WEIGHTS", raising=False)
+        else:
+            monkeypatch.setenv("ALTO_HOST_WEIGHTS", weights)
         e = eng.Engine.from_state(st)
         ql, rl = e.request_len(), e.response_len()
         n, status, host = _answer(e, [frames[i] for i in range(b)], fill=0x11)
@@ -237,7 +245,7 @@ def test_every_schedule_returns_identical_bytes(gpu, svc, eng, monkeypatch):
         assert np.array_equal(dev, host) and (host[3] == 0x11).all()
         if want is None:
             want = host
-        assert np.array_equal(host, want), (overlap, groups, host_groups)
+        assert np.array_equal(host, want), (overlap, groups, host_groups, weights)
         e.close()
 
 
