@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 #include <dlfcn.h>
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <cstdio>
 #include <cstring>
@@ -255,7 +256,7 @@ struct Engine {
   double kernel_ms[5] = {0, 0, 0, 0, 0};  // validate, limb split + zeroing, scan, pack, tail
   long long kernel_batches = 0;
   CUtensorMap map_db, map_ub;
-  int last_launches = 0;
+  std::atomic<int> last_launches{0};  // written by whichever thread enqueued the latest batch (a serving loop's too)
   bool use_graphs = false;  // replay captured launch sequences (alto_engine_set_graphs)
   bool overlap = true;      // the two-stream schedule of a batch (ALTO_OVERLAP=0 runs it on one stream)
   int groups = 2;           // column groups of the scan and tail of a device batch (ALTO_GROUPS: 1, 2, 4 or 8)
@@ -1560,7 +1561,7 @@ int alto_kernel_times(void *p, double *ms, long long *batches, int reset) {
   return 0;
 }
 
-int alto_last_launches(const void *p) { return p ? static_cast<const Engine *>(p)->last_launches : 0; }
+int alto_last_launches(const void *p) { return p ? static_cast<const Engine *>(p)->last_launches.load() : 0; }
 
 int alto_engine_set_tuning(void *p, const int32_t *entries, size_t n) {
   Engine *e = static_cast<Engine *>(p);

@@ -186,7 +186,10 @@ int alto_answer_device_noalloc(void *engine, const uint8_t *d_req, size_t req_st
  *   alto_server_free       answers everything queued, then stops the threads and frees the contexts.
  * alto_server_new_loopback builds the same loop without an engine: batches are answered on the host after
  * service_us microseconds by a deterministic function of the frame, to test queueing and batching without a
- * device.  Both have no counterpart in the reference's C ABI. */
+ * device.  Both have no counterpart in the reference's C ABI.
+ * The loop answers in batch contexts of its own, so while it runs, one other thread may still call alto_answer,
+ * alto_answer_device or alto_enqueue_device on the same engine; alto_engine_set_tuning, alto_engine_set_graphs,
+ * the ingest calls and alto_engine_free must wait until alto_server_free has returned. */
 void *alto_server_new(void *engine, size_t max_batch, size_t queue_cap, int slots);
 void *alto_server_new_loopback(size_t request_len, size_t response_len, size_t max_batch, size_t queue_cap, int slots,
                                double service_us);
