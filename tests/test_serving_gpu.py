@@ -38,3 +38,31 @@ def test_each_result_is_the_same_alone_and_in_the_mix(gpu, svc, eng):
     assert stats["p50_ms"] > 0 and stats["p99_ms"] >= stats["p50_ms"]
     s.close()
     e.close()
+
+
+@pytest.mark.timeout(300, method="thread")
+def test_direct_answers_beside_a_running_loop(gpu, svc, eng):
+    # the loop answers in batch contexts of its own, so alto_answer on the same engine may run beside it
+    from altopir_b200 import server as srv
+    p = svc.params(2048, 4096)
+    st = svc.SyntheticState.make(p, seed=81, full_prefix=True)
+    e = eng.Engine.from_state(st)
+    frames = svc.synthetic_requests(p, 40, seed=82)
+    rl = e.response_len()
+    alone = np.zeros((40, rl), dtype=np.uint8)
+    status = np.full(40, -1, dtype=np.int32)
+    assert e.answer([frames[i] for i in range(40)], alone, status)[0] == 40
+    s = srv.Server(e, max_batch=8, queue_cap=64, slots=2)
+    for rep in range(3):
+        tickets = [s.submit(frames[i]) for i in range(24)]
+        assert all(t >= 0 for t in tickets)
+        direct = np.zeros((16, rl), dtype=np.uint8)
+        dst = np.full(16, -1, dtype=np.int32)
+        assert e.answer([frames[24 + i] for i in range(16)], direct, dst)[0] == 16
+        assert np.array_equal(direct, alone[24:]), rep
+        for i, t in enumerate(tickets):
+            code, resp = s.wait(t)
+            assert code == 0 and np.array_equal(resp, alone[i]), (rep, i)
+    assert s.stats()["failed"] == 0
+    s.close()
+    e.close()
