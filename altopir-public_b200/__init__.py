@@ -48,6 +48,8 @@ def _declare(L):
         "alto_engine_stream": (P, [P]),
         "alto_kernel_times": (I, [P, c.POINTER(c.c_double), c.POINTER(c.c_longlong), I]),
         "alto_engine_set_graphs": (I, [P, I]),
+        "alto_engine_set_lanes": (I, [P, I]),
+        "alto_engine_fence": (I, [P]),
         "alto_engine_set_tuning": (I, [P, P, S]),
         "alto_answer_device_noalloc": (I, [P, P, S, S, P, S, P]),
         "alto_answer_device_parts": (I, [P, P, S, S, PP, S, S, S, c.POINTER(I)]),
@@ -87,7 +89,8 @@ EXPORTS = (
     "sw_amx_init", "sw_alloc_zeroed", "sw_alloc", "sw_free", "sw_tile_db", "sw_pack_build", "alto_engine_new",
     "alto_engine_free", "alto_request_len", "alto_response_len", "alto_answer", "alto_last_error",
     "alto_answer_device", "alto_last_launches", "alto_enqueue_device", "alto_engine_sync", "alto_engine_stream",
-    "alto_kernel_times", "alto_engine_set_graphs", "alto_engine_set_tuning", "alto_answer_device_noalloc",
+    "alto_kernel_times", "alto_engine_set_graphs", "alto_engine_set_lanes", "alto_engine_fence",
+    "alto_engine_set_tuning", "alto_answer_device_noalloc",
     "alto_answer_device_parts", "alto_ipc_export", "alto_ipc_import", "alto_ipc_release", "alto_server_new",
     "alto_server_new_loopback",
     "alto_server_submit", "alto_server_wait", "alto_server_stats", "alto_server_free", "alto_engine_new_empty",

@@ -184,6 +184,7 @@ bool upload_tiled(uint8_t *dst, const uint8_t *src, size_t pitch, size_t nrows, 
 // then misses on every box); chunks of 32768 records keep a box inside a few pages.  32768 is also the longest
 // reduction an int32 limb sum can take exactly, so a scan unit never spans more than one chunk.
 constexpr size_t kRecordChunk = 32768;
+constexpr int kMaxLanes = 4;  // batch contexts alto_enqueue_device can rotate through
 
 // ------------------------------------------------------------------------------------------- engine
 // The device resources of one batch in flight: its stream, per-batch scratch (grown on demand) and error word.
@@ -244,6 +245,12 @@ struct Engine {
   uint8_t *d_db = nullptr, *d_ub = nullptr, *d_prefix = nullptr;
   uint32_t *d_that = nullptr, *d_tw = nullptr;
   Batch main;
+  // alto_enqueue_device rotates through `lanes` batch contexts -- main, lane[0], lane[1], ... -- so that consecutive
+  // asynchronous batches overlap on the device (alto_engine_set_lanes); lanes_made contexts exist, lane_next is the
+  // context of the next batch, and ev_lane[k] marks lane k's stream for alto_engine_fence
+  Batch lane[kMaxLanes - 1];
+  int lanes = 1, lanes_made = 1, lane_next = 0;
+  cudaEvent_t ev_lane[kMaxLanes] = {};
   // per call: before the uploads, after the downloads; the query words upload on st_copy
   cudaEvent_t ev_begin = nullptr, ev_end = nullptr, ev_keys = nullptr, ev_queries = nullptr, ev_zkeys = nullptr;
   cudaStream_t st_copy = nullptr;
@@ -399,10 +406,16 @@ void destroy_batch(Batch *b) {
   b->d_err = b->h_err = nullptr;
 }
 
+Batch *lane_batch(Engine *e, int k) { return k == 0 ? &e->main : &e->lane[k - 1]; }
+
 void destroy(Engine *e) {
   if (!e) return;
   if (e->dev >= 0) cudaSetDevice(e->dev);
-  if (e->main.st) cudaStreamSynchronize(e->main.st);
+  for (int k = 0; k < e->lanes_made; ++k) {
+    Batch *b = lane_batch(e, k);
+    if (b->st) cudaStreamSynchronize(b->st);
+    if (b->side) cudaStreamSynchronize(b->side);
+  }
   cudaFree(e->d_db);
   cudaFree(e->d_ub);
   cudaFree(e->d_prefix);
@@ -417,6 +430,9 @@ void destroy(Engine *e) {
   for (auto &set : e->marks)
     for (cudaEvent_t &ev : set)
       if (ev) cudaEventDestroy(ev);
+  for (int k = e->lanes_made - 1; k >= 1; --k) destroy_batch(&e->lane[k - 1]);
+  for (cudaEvent_t ev : e->ev_lane)
+    if (ev) cudaEventDestroy(ev);
   destroy_batch(&e->main);
   delete e;
 }
@@ -957,25 +973,37 @@ bool copy_runs(size_t items, size_t width, SrcAt src_at, DstAt dst_at, cudaMemcp
 
 // Waits for the engine's stream, folds pending timing marks into the totals and checks (then clears) the device
 // error word.
-// After the main batch's stream has passed a copy of its error word into the pinned mirror: false (and the word
-// reset) when a kernel wait timed out.
-bool check_error_word(Engine *e) {
-  const uint32_t err = *e->main.h_err;
+// After a batch's stream has passed a copy of its error word into the pinned mirror: false (and the word reset)
+// when a kernel wait timed out.
+bool check_batch_error(Batch *b) {
+  const uint32_t err = *b->h_err;
   if (err) {
-    ALTO_CK(cudaMemsetAsync(e->main.d_err, 0, sizeof(uint32_t), e->main.st));
-    ALTO_CK(cudaStreamSynchronize(e->main.st));
+    ALTO_CK(cudaMemsetAsync(b->d_err, 0, sizeof(uint32_t), b->st));
+    ALTO_CK(cudaStreamSynchronize(b->st));
+    *b->h_err = 0;
     char buf[96];
     snprintf(buf, sizeof buf, "a kernel wait timed out (device error word 0x%x)", err);
     set_error(buf);
     return false;
   }
-  return accumulate_pending(e);
+  return true;
 }
 
+// The same for the main batch, then the pending timing marks folded into the totals.
+bool check_error_word(Engine *e) { return check_batch_error(&e->main) && accumulate_pending(e); }
+
+// Waits for every batch context of the engine and checks (then clears) each one's error word.
 bool sync_engine(Engine *e) {
+  bool ok = true;
+  for (int k = e->lanes_made - 1; k >= 1; --k) {
+    Batch *b = &e->lane[k - 1];
+    ALTO_CK(cudaMemcpyAsync(b->h_err, b->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, b->st));
+    ALTO_CK(cudaStreamSynchronize(b->st));
+    ok = check_batch_error(b) && ok;
+  }
   ALTO_CK(cudaMemcpyAsync(e->main.h_err, e->main.d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->main.st));
   ALTO_CK(cudaStreamSynchronize(e->main.st));
-  return check_error_word(e);
+  return check_error_word(e) && ok;
 }
 
 bool finish(Engine *e, double *stage_ms) {
@@ -1175,7 +1203,10 @@ namespace {
 // cols bytes each) into the database tiles, through a 64 MB device staging buffer: per pass, whole 128-record
 // blocks of the tile grid (the first and last may be partly covered, their other records kept).
 bool load_records(Engine *e, const uint8_t *records, size_t pitch, size_t first, size_t count) {
-  ALTO_CK(cudaStreamSynchronize(e->main.st));  // batches already enqueued read the database
+  for (int k = 0; k < e->lanes_made; ++k) {  // batches already enqueued read the database
+    ALTO_CK(cudaStreamSynchronize(lane_batch(e, k)->st));
+    ALTO_CK(cudaStreamSynchronize(lane_batch(e, k)->side));
+  }
   const size_t per = std::max<size_t>(128, (size_t(64) << 20) / e->cols / 128 * 128);  // records per pass
   uint8_t *stage = nullptr;
   ALTO_CK(cudaMalloc(&stage, per * e->cols));
@@ -1529,10 +1560,12 @@ int alto_enqueue_device(void *p, const uint8_t *d_req, size_t req_stride, size_t
   e->last_launches = 0;
   if (!b) return 0;
   if (!e->tail_ok) return -3;
-  if (cudaSetDevice(e->dev) != cudaSuccess || !ensure_capacity(e, &e->main, b)) return -4;
-  if (!enqueue_batch(e, &e->main, d_req, req_stride, b, d_out, out_stride, false)) return -4;
+  Batch *bt = lane_batch(e, e->lane_next);
+  e->lane_next = (e->lane_next + 1) % e->lanes;
+  if (cudaSetDevice(e->dev) != cudaSuccess || !ensure_capacity(e, bt, b)) return -4;
+  if (!enqueue_batch(e, bt, d_req, req_stride, b, d_out, out_stride, false)) return -4;
   if (d_status &&
-      cudaMemcpyAsync(d_status, e->main.d_status, b * sizeof(int), cudaMemcpyDeviceToDevice, e->main.st) != cudaSuccess) {
+      cudaMemcpyAsync(d_status, bt->d_status, b * sizeof(int), cudaMemcpyDeviceToDevice, bt->st) != cudaSuccess) {
     set_error("status copy failed");
     return -4;
   }
@@ -1566,22 +1599,60 @@ int alto_last_launches(const void *p) { return p ? static_cast<const Engine *>(p
 int alto_engine_set_tuning(void *p, const int32_t *entries, size_t n) {
   Engine *e = static_cast<Engine *>(p);
   if (!e || (n && !entries)) return -1;
-  if (cudaSetDevice(e->dev) != cudaSuccess || cudaStreamSynchronize(e->main.st) != cudaSuccess) return -4;
+  if (cudaSetDevice(e->dev) != cudaSuccess || !sync_engine(e)) return -4;
   e->tuning.clear();
   for (size_t i = 0; i < n; ++i)
     e->tuning.push_back({entries[5 * i], entries[5 * i + 1], entries[5 * i + 2], entries[5 * i + 3],
                          entries[5 * i + 4]});
   std::sort(e->tuning.begin(), e->tuning.end(), [](const TuneEntry &a, const TuneEntry &b) { return a.b_max < b.b_max; });
-  clear_graphs(&e->main);  // captured sequences follow the old plans
+  for (int k = 0; k < e->lanes_made; ++k) clear_graphs(lane_batch(e, k));  // captured sequences follow old plans
   return 0;
 }
 
 int alto_engine_set_graphs(void *p, int on) {
   Engine *e = static_cast<Engine *>(p);
   if (!e) return -1;
-  if (cudaSetDevice(e->dev) != cudaSuccess || cudaStreamSynchronize(e->main.st) != cudaSuccess) return -4;
+  if (cudaSetDevice(e->dev) != cudaSuccess || !sync_engine(e)) return -4;
   e->use_graphs = on != 0;
-  if (!e->use_graphs) clear_graphs(&e->main);
+  if (!e->use_graphs)
+    for (int k = 0; k < e->lanes_made; ++k) clear_graphs(lane_batch(e, k));
+  return 0;
+}
+
+int alto_engine_set_lanes(void *p, int lanes) {
+  Engine *e = static_cast<Engine *>(p);
+  if (!e || lanes < 1 || lanes > kMaxLanes) return -1;
+  if (cudaSetDevice(e->dev) != cudaSuccess || !sync_engine(e)) return -4;
+  for (int k = 0; k < kMaxLanes; ++k)
+    if (!e->ev_lane[k] && cudaEventCreateWithFlags(&e->ev_lane[k], cudaEventDisableTiming) != cudaSuccess) {
+      set_error("lane event", cudaGetLastError());
+      return -4;
+    }
+  while (e->lanes_made < lanes) {
+    if (!init_batch(&e->lane[e->lanes_made - 1], false)) return -4;
+    ++e->lanes_made;
+  }
+  e->lanes = lanes;
+  e->lane_next = 0;
+  return 0;
+}
+
+int alto_engine_fence(void *p) {
+  Engine *e = static_cast<Engine *>(p);
+  if (!e) return -1;
+  if (e->lanes_made == 1) return 0;
+  if (cudaSetDevice(e->dev) != cudaSuccess) return -4;
+  for (int k = 0; k < e->lanes_made; ++k)
+    if (cudaEventRecord(e->ev_lane[k], lane_batch(e, k)->st) != cudaSuccess) {
+      set_error("lane fence", cudaGetLastError());
+      return -4;
+    }
+  for (int j = 0; j < e->lanes_made; ++j)
+    for (int k = 0; k < e->lanes_made; ++k)
+      if (k != j && cudaStreamWaitEvent(lane_batch(e, j)->st, e->ev_lane[k], 0) != cudaSuccess) {
+        set_error("lane fence", cudaGetLastError());
+        return -4;
+      }
   return 0;
 }
 

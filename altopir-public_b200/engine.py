@@ -204,6 +204,16 @@ class Engine:
         if lib().alto_engine_set_graphs(self.ptr, int(on)) < 0:
             raise EngineError(last_error())
 
+    def set_lanes(self, lanes):
+        """alto_engine_set_lanes: enqueue_device rotates through `lanes` batch contexts (1..4)."""
+        if lib().alto_engine_set_lanes(self.ptr, int(lanes)) < 0:
+            raise EngineError(last_error())
+
+    def fence(self):
+        """alto_engine_fence: every lane's stream waits for the others' work enqueued so far (no host wait)."""
+        if lib().alto_engine_fence(self.ptr) < 0:
+            raise EngineError(last_error())
+
     def last_launches(self):
         return lib().alto_last_launches(self.ptr)
 

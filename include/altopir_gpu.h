@@ -130,6 +130,17 @@ int alto_enqueue_device(void *engine, const uint8_t *d_req, size_t req_stride, s
  * check (the device error word is cleared). */
 int alto_engine_sync(void *engine);
 
+/* Batch lanes of alto_enqueue_device (default 1).  With 2..4 lanes consecutive calls rotate through that many batch
+ * contexts -- the engine's own, then contexts with streams and scratch of their own, made on first use -- so that
+ * a batch overlaps the previous one on the device (its tail, and its GEMMs' last partial round of units).  Batches
+ * in flight at once must not write the same outputs or statuses.  alto_engine_set_lanes waits for the engine first
+ * and returns 0, -1 (lanes outside 1..4) or -4.  alto_engine_sync waits for every lane.  alto_engine_fence makes
+ * every lane's stream wait for the work enqueued so far on every other lane, without a host wait, so that work
+ * ordered on alto_engine_stream after a fence follows every lane's batches (and batches enqueued after a fence
+ * follow work put on that stream before it); 0, -1 or -4. */
+int alto_engine_set_lanes(void *engine, int lanes);
+int alto_engine_fence(void *engine);
+
 /* The cudaStream_t the engine launches its kernels on (for events and stream ordering in the caller). */
 void *alto_engine_stream(void *engine);
 

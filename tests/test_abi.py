@@ -128,3 +128,11 @@ def test_ingest_entry_points_reject_bad_arguments_without_a_device(svc):
         assert pkg.last_error()
     assert L.alto_engine_load_records(None, ptr, 4096, 0, 1) == -1
     assert L.alto_engine_load_file(None, b"/nonexistent", 0) == -1
+
+
+def test_lane_entry_points_reject_a_null_engine_without_a_device():
+    import altopir_b200 as pkg
+    L = pkg.lib()
+    assert L.alto_engine_set_lanes(None, 2) == -1
+    assert L.alto_engine_fence(None) == -1
+    assert L.alto_engine_sync(None) == -1

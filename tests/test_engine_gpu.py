@@ -300,3 +300,51 @@ def test_other_key_counts_and_row1_moduli_match_oracle(gpu, oracle, svc, eng, tg
     r, ost, oout = oracle.answer(st, [frames[i] for i in range(6)])
     assert n_ok == r == 6 and np.array_equal(out, oout)
     e.close()
+
+
+def test_batch_lanes_return_the_same_bytes(gpu, svc, eng):
+    # alto_engine_set_lanes: consecutive enqueue_device batches rotate through 1..4 batch contexts and overlap on the
+    # device; every batch's responses and statuses equal alto_answer's, with and without graph replay, and work put
+    # on the engine's stream after alto_engine_fence (no host wait in between) sees every lane's results
+    import torch
+    p = svc.params(4096, 32768)
+    st = svc.SyntheticState.make(p, seed=51)
+    e = eng.Engine.from_state(st)
+    ql, rl = e.request_len(), e.response_len()
+    stride = (7 + ql + 15) // 16 * 16
+    batches = []
+    for j, b in enumerate((24, 17, 32)):
+        frames = svc.synthetic_requests(p, b, seed=60 + j)
+        if j == 1:
+            frames[2, 9:13] = 0xFF  # y[0] >= Q: status 3
+        want = np.full((b, rl), 0x11, dtype=np.uint8)
+        wst = np.full(b, -1, dtype=np.int32)
+        e.answer([frames[i] for i in range(b)], want, wst)
+        slots = torch.zeros((b, stride), dtype=torch.uint8, device="cuda")
+        slots[:, 7:7 + ql] = torch.from_numpy(frames).cuda()
+        batches.append((b, slots, want, wst))
+    assert batches[1][3][2] == 3
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(e.stream())
+    for graphs in (False, True):
+        e.set_graphs(graphs)
+        for lanes in (1, 2, 3, 4):
+            e.set_lanes(lanes)
+            for rep in range(2):
+                outs = [torch.full((b, rl), 0x11, dtype=torch.uint8, device="cuda") for b, *_ in batches]
+                stats = [torch.full((b,), -1, dtype=torch.int32, device="cuda") for b, *_ in batches]
+                torch.cuda.synchronize()
+                for (b, slots, _, _), out, s in zip(batches, outs, stats):
+                    e.enqueue_device(slots.data_ptr(), stride, b, out.data_ptr(), rl, s.data_ptr())
+                e.fence()
+                with torch.cuda.stream(stream):
+                    copies = [o.clone() for o in outs]
+                    stat_copies = [s.clone() for s in stats]
+                stream.synchronize()
+                for (b, _, want, wst), c, sc in zip(batches, copies, stat_copies):
+                    assert np.array_equal(c.cpu().numpy(), want), (graphs, lanes, rep, b)
+                    assert list(sc.cpu().numpy()) == list(wst), (graphs, lanes, rep, b)
+                e.sync()
+    e.set_lanes(1)
+    e.set_graphs(False)
+    e.close()
