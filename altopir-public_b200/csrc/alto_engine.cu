@@ -1668,6 +1668,52 @@ int alto_synthetic_db_col_device(uint8_t *d_db, size_t ld, size_t rows, size_t c
   return 0;
 }
 
+int alto_engine_fill_synthetic(void *p) {
+  Engine *e = static_cast<Engine *>(p);
+  if (!e) {
+    set_error("alto_engine_fill_synthetic: NULL engine");
+    return -1;
+  }
+  if (cudaSetDevice(e->dev) != cudaSuccess) return -4;
+  for (int k = 0; k < e->lanes_made; ++k) {  // batches already enqueued read the database
+    if (cudaStreamSynchronize(lane_batch(e, k)->st) != cudaSuccess ||
+        cudaStreamSynchronize(lane_batch(e, k)->side) != cudaSuccess) {
+      set_error("alto_engine_fill_synthetic", cudaGetLastError());
+      return -4;
+    }
+  }
+  const size_t tiles = e->db_mts * e->db_kbs, threads = tiles * 512;
+  alto::synthetic_tiles_kernel<<<(unsigned)((threads + 255) / 256), 256>>>(e->d_db, e->db_kbs, tiles, e->rows,
+                                                                            e->cols);
+  cudaError_t err = cudaGetLastError();
+  if (err == cudaSuccess) err = cudaStreamSynchronize(0);
+  if (err != cudaSuccess) {
+    set_error("alto_engine_fill_synthetic", err);
+    return -4;
+  }
+  return 0;
+}
+
+int alto_synthetic_requests_device(uint8_t *d_slots, size_t stride, size_t lead, size_t b, size_t rows, size_t tg_n,
+                                   uint64_t seed, uint64_t first_client) {
+  if (!d_slots || (lead + 9) % 4 || stride % 4 || stride < lead + 9 + 4 * (2 * tg_n + rows) || b > 65535 ||
+      tg_n > 0xffffffffu || (reinterpret_cast<uintptr_t>(d_slots) & 3)) {
+    set_error("alto_synthetic_requests_device: bad arguments");
+    return -1;
+  }
+  if (!b) return 0;
+  const size_t words = 2 * tg_n + rows;
+  const dim3 grid((unsigned)((words + 255) / 256), (unsigned)b);
+  alto::synthetic_requests_kernel<<<grid, 256>>>(d_slots, stride, lead, rows, tg_n, seed, first_client);
+  cudaError_t err = cudaGetLastError();
+  if (err == cudaSuccess) err = cudaStreamSynchronize(0);
+  if (err != cudaSuccess) {
+    set_error("alto_synthetic_requests_device", err);
+    return -4;
+  }
+  return 0;
+}
+
 }  // extern "C"
 
 // ============================================================================================ allocation-free answer
@@ -1785,6 +1831,7 @@ bool enqueue_noalloc(Engine *e, uint8_t *scratch, const NoAllocLayout &l, const 
   t.o_count = (int)e->outputs;
   ALTO_CK(alto::launch_tail(t, b, st));
   ALTO_CK(cudaMemcpyAsync(d_status, status, b * sizeof(int), cudaMemcpyDeviceToDevice, st));
+  e->last_launches = 6;  // validate, two limb splits, scan, pack, tail
   return true;
 }
 
@@ -1798,6 +1845,7 @@ extern "C" int alto_answer_device_noalloc(void *p, const uint8_t *d_req, size_t 
     set_error("bad arguments");
     return -1;
   }
+  e->last_launches = 0;
   if (!b) return 0;
   if (!e->tail_ok) return -3;
   const NoAllocLayout l = noalloc_layout(e, b);

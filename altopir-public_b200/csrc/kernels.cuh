@@ -395,6 +395,57 @@ __global__ void synthetic_db_kernel(uint8_t *db, size_t ld, size_t rows, size_t 
   *reinterpret_cast<uint32_t *>(db + c * ld + r0) = word;
 }
 
+// The same records written straight into the database's tile layout: tile (mt, kb) at (mt * kbs + kb) * 16 KB, its
+// row r = column 128 mt + r, byte k of a row = record 128 kb + k.  Columns 2c and 2c + 1 are the two bytes of one
+// splitmix64 output, so a thread takes a pair of tile rows and 16 records: 16 finaliser evaluations fill two 16-byte
+// words.  Records >= rows and columns >= cols are zero (cols is even).
+__global__ void synthetic_tiles_kernel(uint8_t *db, size_t kbs, size_t tiles, size_t rows, size_t cols) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t tile = idx >> 9;  // 64 row pairs x 8 groups of 16 records per tile
+  if (tile >= tiles) return;
+  const int rp = (int)((idx >> 3) & 63), g = (int)(idx & 7);
+  const size_t mt = tile / kbs, kb = tile - mt * kbs;
+  const size_t col = mt * 128 + 2 * rp, rec0 = kb * 128 + g * 16;
+  uint32_t lo[4] = {0, 0, 0, 0}, hi[4] = {0, 0, 0, 0};
+  if (col < cols) {
+    const uint64_t step = (col / 2 + 1) * 0x9e3779b97f4a7c15ull;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const uint64_t row = rec0 + k;
+      if (row < rows) {
+        const uint64_t s0 = 0x416c746f504952ull ^ (0xd1b54a32d192ed03ull * (row + 1));
+        const uint32_t v = (uint32_t)(splitmix_finalise(s0 + step) % 65535ull);
+        lo[k >> 2] |= (v & 0xffu) << (8 * (k & 3));
+        hi[k >> 2] |= (v >> 8) << (8 * (k & 3));
+      }
+    }
+  }
+  uint8_t *base = db + tile * 16384 + (size_t)(2 * rp) * 128 + g * 16;
+  *reinterpret_cast<uint4 *>(base) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+  *reinterpret_cast<uint4 *>(base + 128) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+}
+
+// Seeded synthetic request frames (the bytes alto_synthetic_request writes on the host) straight into device slots:
+// frame c at slots + c * stride + lead.  Client s = seed ^ 0xd1b54a32d192ed03 (client + 1) draws word i of its keys
+// and query from splitmix64 counter s: key words uniform in [0, Q) by a multiply-high of the output's top half,
+// query words the output's top half.  The caller puts the key words on a 4-byte boundary ((lead + 9) % 4 == 0 and
+// stride % 4 == 0).  Grid: (word blocks, b); thread 0 of block 0 also writes the 9-byte header.
+__global__ void synthetic_requests_kernel(uint8_t *slots, size_t stride, size_t lead, size_t rows, size_t tg_n,
+                                          uint64_t seed, uint64_t first_client) {
+  const uint64_t client = first_client + blockIdx.y;
+  const uint64_t s = seed ^ (0xd1b54a32d192ed03ull * (client + 1));
+  uint8_t *f = slots + (size_t)blockIdx.y * stride + lead;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x, keys = 2 * tg_n;
+  if (i == 0) {
+    f[0] = 0;
+    for (int b = 0; b < 4; ++b) f[1 + b] = f[5 + b] = (uint8_t)(tg_n >> (8 * b));
+  }
+  if (i >= keys + rows) return;
+  const uint64_t x = splitmix_finalise(s + (i + 1) * 0x9e3779b97f4a7c15ull);
+  const uint32_t v = i < keys ? (uint32_t)(((x >> 32) * kQ) >> 32) : (uint32_t)(x >> 32);
+  reinterpret_cast<uint32_t *>(f + 9)[i] = v;
+}
+
 }  // namespace alto
 
 namespace alto {

@@ -109,12 +109,23 @@ class Engine:
         if r < 0:
             raise EngineError(f"engine error {r}: {last_error()}")
 
+    def fill_synthetic(self):
+        """alto_engine_fill_synthetic: the whole database becomes the synthetic records, generated on the device."""
+        r = lib().alto_engine_fill_synthetic(self.ptr)
+        if r < 0:
+            raise EngineError(f"engine error {r}: {last_error()}")
+
     @staticmethod
     def from_state(st, threads=1, tile=True):
         """Prepared::engine (src/service.rs:159-170) for a service.SyntheticState.  With tile=False no tiled copy
         is made (this engine reads the column-order database and never the tiled one), which halves the host
         memory of very large databases."""
         p = st.p
+        if st.db_col is None:  # a state without a host database: the synthetic records are generated on the device
+            e = Engine.empty(p.rows, p.record_bytes, st.ub, p.n, p.tg, st.prefixes, p.row1_off, 1 << p.q1_bits,
+                             p.q1_bits, st.that, st.inv_table, Q, threads)
+            e.fill_synthetic()
+            return e
         if tile:
             tiled = TiledDb(st.db_col, st.db_col.shape[1], p.rows, p.record_bytes, threads)
         else:

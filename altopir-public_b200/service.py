@@ -168,6 +168,15 @@ def synthetic_requests(p: Params, b, seed, first_client=0):
     return out
 
 
+def synthetic_requests_device(p: Params, b, seed, d_slots, stride, lead=7, first_client=0):
+    """The frames of synthetic_requests written straight into device memory: frame c at d_slots + c * stride +
+    lead (alto_synthetic_requests_device)."""
+    r = lib().alto_synthetic_requests_device(ctypes.c_void_p(d_slots), stride, lead, b, p.rows, p.count, seed,
+                                             first_client)
+    if r < 0:
+        raise RuntimeError(f"alto_synthetic_requests_device: {lib().alto_last_error().decode()}")
+
+
 def _pow(a, e):
     return pow(int(a), int(e), Q)
 
@@ -202,9 +211,10 @@ class SyntheticState:
     inv_table: np.ndarray = field(repr=False)
 
     @staticmethod
-    def make(p: Params, seed=1, full_prefix=False, keep_values=True):
+    def make(p: Params, seed=1, full_prefix=False, keep_values=True, host_db=True):
+        """host_db=False leaves db_col None: Engine.from_state then generates the same records on the device."""
         cols, count, outputs = p.record_bytes, p.count, p.instances
-        db = synthetic_db_col(p.rows, cols)
+        db = synthetic_db_col(p.rows, cols) if host_db else None
         U = uniform_u32(cols * count, Q, seed * 0x1000193 + 1).reshape(cols, count)
         ub = np.empty(4 * cols * count, dtype=np.int8)
         lib().alto_pack_encode(_ptr(ub), _ptr(U), cols, count, threads())

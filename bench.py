@@ -1,21 +1,27 @@
 #!/usr/bin/env python
-"""Throughput of the AltoPIR answer path on B200: byte-exact QPS of 128-query batches on a 1 GiB database
-(32,768 records x 32 KB), the configuration the reference's headline batch numbers are quoted on.
+"""Throughput of the AltoPIR answer path on B200: byte-exact QPS of answer batches.  The headline is 128-query
+batches on a 1 GiB database (32,768 records x 32 KB), the configuration of the reference's headline batch numbers;
+the same JSON line carries the 8 GiB (B = 1, 128, 1024) and 64 GiB (B = 128, 1024) databases under `configs`.
 
 One step = one batch of --batch queries through the whole answer path (validate, limb split, scan, pack, tail).
-  value : device-resident throughput -- frames already in HBM, batches enqueued back to back on the engine's
-          stream (alto_enqueue_device, the launch sequence replayed as a CUDA graph), timed with CUDA events on that
-          stream, max over ranks.  The per-kernel durations behind `kernels` and `roofline` come from a second pass
-          of the same batches launched directly, each stage bracketed by CUDA events on the engine's stream.
-  e2e   : the same metric through the reference-facing C ABI (alto_answer) with pinned HOST frames and output
-          buffers: every step uploads its frames and downloads its responses inside the timed region.
+Every measurement times blocks of exactly --steps steps with CUDA events (a barrier and a synchronisation on both
+sides of each block, max over ranks), back to back until the blocks add up to at least one second of device time and
+at least five blocks; the figures are over all blocks.
+  value : device-resident throughput -- frames already in HBM, batches enqueued back to back (alto_enqueue_device
+          rotating through two batch contexts, each replaying its launch sequence as a CUDA graph), timed on the
+          engine's stream.  `kernels` and `roofline` come from a second pass of the same batches launched directly on
+          one context, each stage bracketed by CUDA events on the engine's stream.
+  e2e   : the same metric through the reference-facing C ABI (alto_answer) with pinned HOST frames and output buffers:
+          every step uploads its frames and downloads its responses inside the timed region.
 Every rank answers its own batches on its own GPU (the answer path needs no exchange between GPUs: replicas, weak
-scaling).  `--impl reference` runs the reference's CPU engine (src/amx_kernels.cpp compiled from its own sources,
-AMX when the host has it) on the same workload, on rank 0 only.
+scaling).  `--impl reference` runs the reference's CPU engine (src/amx_kernels.cpp compiled from its own sources by
+oracle/Makefile, AMX when the host has it) on the same workload, on rank 0 only, with inputs built by the oracle's
+generators so that the engine library is never loaded in that arm.
 """
 import argparse
 import ctypes
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -29,19 +35,29 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "QPS (byte-exact) at 1/8/64 GB DB, batched vs per-query on 1 B200; p50/p99 ms"
+MIN_TIMED_S = 1.0   # device time every measurement accumulates over its blocks of --steps steps
+MIN_BLOCKS = 5
+# The reference's published QPS for the same record size on 16 cores of a Xeon Silver 4514Y (README: "Benchmark
+# without the network", batch 128 at 1 GB, and the Results table at 8 and 64 GB).
+PUBLISHED_QPS = {32768: (1986.3, "README bench, 1 GB, batch 128: 64.44 ms median"),
+                 262144: (492.0, "README Results table, 8 GB"),
+                 2097152: (70.2, "README Results table, 64 GB")}
+# The larger configurations measured beside the headline (rows, batch sizes, single queries timed for the plain path).
+SUB_CONFIGS = ((262144, (1, 128, 1024), 32), (2097152, (128, 1024), 8))
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=400)
-    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--rows", type=int, default=32768)
     ap.add_argument("--record-bytes", type=int, default=32768)
     ap.add_argument("--batch", type=int, default=128)
     ap.add_argument("--plain-queries", type=int, default=128, help="single-query launches timed for the plain path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true", help="skip the 8 GiB and 64 GiB configurations")
     ap.add_argument("--serve", type=str, default=None,
                     help="serving mode: comma-separated offered rates in QPS (open-loop Poisson arrivals)")
     ap.add_argument("--serve-seconds", type=float, default=3.0)
@@ -52,20 +68,30 @@ def parse():
     ap.add_argument("--shard", action="store_true",
                     help="column sharding: the ranks split the outputs of one engine state and answer every batch "
                          "together (strong scaling); the default runs one whole engine per rank (replicas)")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
-def config_dict(a):
-    gib = a.rows * a.record_bytes / 2 ** 30
-    return {"workload": f"answer {a.batch}-query batches over a {gib:g} GiB database ({a.rows} records x "
-                        f"{a.record_bytes} B), synthetic records of the reference generator, seeded keys/queries",
-            "rows": a.rows, "record_bytes": a.record_bytes, "batch": a.batch, "n": 2048, "tg": 4,
-            "l2": "inputs larger than L2: every step streams the 1 GiB database and the 1 GiB packing matrix"}
+def l2_note(rows, record_bytes, count=8192):
+    db, pm = rows * record_bytes, 4 * record_bytes * count
+    return (f"inputs larger than L2 (126 MB): every step streams the {db / 2**30:g} GiB database and the "
+            f"{pm / 2**30:g} GiB packing matrix from HBM")
+
+
+def config_dict(a, rows=None, batch=None):
+    """The workload; identical in both arms for the same arguments."""
+    rows = a.rows if rows is None else rows
+    batch = a.batch if batch is None else batch
+    gib = rows * a.record_bytes / 2 ** 30
+    return {"workload": f"answer {batch}-query batches over a {gib:g} GiB database ({rows} records x "
+                        f"{a.record_bytes} B): synthetic records of the reference generator, seeded keys and queries",
+            "rows": rows, "record_bytes": a.record_bytes, "batch": batch, "n": 2048, "tg": 4,
+            "l2": l2_note(rows, a.record_bytes)}
 
 
 # ------------------------------------------------------------------------------------------------ clocks
 class ClockSampler:
-    """nvidia-smi clock/throttle samples every 200 ms while running."""
+    """nvidia-smi clock/throttle samples every 200 ms while running; summary() keeps the samples taken inside the
+    marked (timed) intervals."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -99,17 +125,22 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
-    def summary(self):
-        inside = [s for t, s in self.samples if any(a - 0.25 <= t <= b + 0.25 for a, b in self.marks)]
-        use = inside or [s for _, s in self.samples]
+    def summary(self, marks=None):
+        marks = self.marks if marks is None else marks
+        inside = [s for t, s in self.samples if any(a <= t <= b for a, b in marks)]
+        use = inside or [s for t, s in self.samples if any(a - 0.25 <= t <= b + 0.25 for a, b in marks)]
         if not use:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no nvidia-smi samples"], "samples": 0}
-        sm = [float(s[1]) for s in use if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in use if s[2].replace(".", "").isdigit()]
+        num = lambda x: x.replace(".", "", 1).isdigit()
+        sm = [float(s[1]) for s in use if num(s[1])]
+        mx = [float(s[2]) for s in use if num(s[2])]
+        pw = [float(s[3]) for s in use if num(s[3])]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for s in use for i in range(4) if len(s) > 5 + i and s[5 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(use), "in_timed_region": bool(inside)}
+                "sm_mhz_min": min(sm) if sm else None, "power_w_median": statistics.median(pw) if pw else None,
+                "reasons": reasons, "samples": len(use), "in_timed_region": bool(inside),
+                "timed_region_s": sum(b - a for a, b in marks)}
 
 
 # ------------------------------------------------------------------------------------------------ helpers
@@ -118,15 +149,41 @@ def measured_peaks():
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             return json.load(f), "measured"
     except OSError:
-        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
 def algorithmic(rows, cols, b, count):
-    """Per-batch algorithmic work of the two limb GEMMs: int8 ops (1 multiply-add = 2) and compulsory bytes."""
+    """Per-batch algorithmic work of the two limb GEMMs: int8 ops (1 multiply-add = 2) and compulsory bytes (the
+    database or packing matrix once, the limb operand once, the u32 results once)."""
     return {
         "scan_gemm": {"ops": 2.0 * cols * rows * 4 * b, "bytes": rows * cols + rows * 4 * b + 4 * b * cols},
         "pack_gemm": {"ops": 2.0 * 4 * cols * count * 4 * b, "bytes": 4 * count * cols + 4 * count * b + 4 * b * cols},
     }
+
+
+def roofline_of(kernel, alg, avg_ms, peaks, peak_src, traffic=None):
+    """Roofline of one GEMM: its bound is the slower of its ops at the int8 peak (2 x the dense bf16 rate of
+    MEASURED_PEAKS.json, burst) and its compulsory bytes at the HBM copy bandwidth; achieved and frac in that unit."""
+    int8_peak = 2.0 * peaks["bf16_tflops"]
+    t_ops = alg["ops"] / (int8_peak * 1e12)
+    t_bytes = alg["bytes"] / (peaks["hbm_gbs"] * 1e9)
+    s = avg_ms * 1e-3
+    if t_ops >= t_bytes:
+        r = {"bound": "tensor", "achieved": alg["ops"] / s / 1e12, "peak": int8_peak, "unit": "TFLOP/s"}
+    else:
+        r = {"bound": "hbm", "achieved": alg["bytes"] / s / 1e9, "peak": peaks["hbm_gbs"], "unit": "GB/s"}
+    r["frac"] = r["achieved"] / r["peak"]
+    r.update({"kernel": kernel, "traffic": traffic, "avg_ms": avg_ms,
+              "peak_source": f"{peak_src}: int8 = 2 x dense bf16 burst ({peaks['bf16_tflops']} TF/s; B200's dense "
+                             f"int8 rate is twice its bf16 rate), HBM = copy bandwidth ({peaks['hbm_gbs']} GB/s); "
+                             "int8 ops counted as 2 per multiply-add",
+              "algorithmic_ops": alg["ops"], "algorithmic_bytes": alg["bytes"],
+              "hbm_view": {"achieved_gbs": alg["bytes"] / s / 1e9, "frac": alg["bytes"] / s / 1e9 / peaks["hbm_gbs"]},
+              "tensor_view": {"achieved_tops": alg["ops"] / s / 1e12, "frac": alg["ops"] / s / 1e12 / int8_peak}})
+    sus = peaks.get("bf16_tflops_sustained")
+    if sus and r["bound"] == "tensor":
+        r["frac_of_sustained"] = r["achieved"] / (2.0 * sus)
+    return r
 
 
 def int8_cublas_tops(torch):
@@ -151,17 +208,17 @@ def int8_cublas_tops(torch):
 
 
 def traffic_from_profile(kernel, rows, record_bytes, batch):
-    """DRAM bytes per batch of `kernel` (summed over its launches in one batch, the unit its CUDA-event timing uses)
-    from the committed ncu capture (profiles/ncu_traffic.json), which covers the default workload only; None for any
-    other configuration."""
-    if (rows, record_bytes, batch) != (32768, 32768, 128):
-        return None
+    """DRAM bytes per batch of `kernel` from the committed ncu capture (profiles/ncu_traffic.json): a one-kernel
+    capture on a smaller database, scaled to this configuration where the file says how; None when it covers
+    neither."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     try:
         with open(path) as f:
-            return json.load(f).get(kernel, {}).get("dram_bytes_per_batch")
+            d = json.load(f).get(kernel, {})
     except OSError:
         return None
+    per = d.get("scaled_to", {}).get(f"{rows}x{record_bytes}x{batch}")
+    return per if per is not None else None
 
 
 # ------------------------------------------------------------------------------------------------ ranks
@@ -183,70 +240,428 @@ def job_qps(world, batch, steps, max_ms):
     return world * batch * steps / (max_ms * 1e-3)
 
 
+def block_count(first_ms, min_s=MIN_TIMED_S, min_blocks=MIN_BLOCKS, max_blocks=5000):
+    """Blocks to time, the first included, so that they add up to at least min_s of device time."""
+    return int(min(max_blocks, max(min_blocks, math.ceil(min_s * 1e3 / max(first_ms, 1e-3)))))
+
+
+def timed_blocks(block, world, barrier, min_s=MIN_TIMED_S, min_blocks=MIN_BLOCKS):
+    """block() runs one block of steps between synchronisations and returns its device time in ms.  Every rank runs
+    the same number of blocks (from the first block's time, max over ranks); returns the per-block times, each the
+    max over ranks."""
+    barrier()
+    times = [max_over_ranks(block(), world)]
+    for _ in range(block_count(times[0], min_s, min_blocks) - 1):
+        barrier()
+        times.append(max_over_ranks(block(), world))
+    return times
+
+
 # ------------------------------------------------------------------------------------------------ reference arm
-def reference_state(a, svc):
-    p = svc.params(a.rows, a.record_bytes)
-    return p, svc.SyntheticState.make(p, seed=1, keep_values=True)
-
-
-def run_reference_cpu(a, svc, orc, st, frames, steps, warmup):
-    """Times the reference engine (or the oracle port when the host cannot run it) on batches of a.batch frames.
+def run_reference_cpu(st, frames, steps, warmup, sample, min_s=0.0, min_blocks=1):
+    """Times the reference engine (or the oracle port when the host cannot run it) on batches of frames (a list of
+    uint8 arrays), in blocks of `steps` batches after `warmup` untimed ones, until the blocks add up to min_s.
     Returns (qps, info, first_out)."""
+    from oracle import oracle as orc
     methods = orc.ref_methods()
     threads = os.cpu_count() or 1
-    fl = [frames[i] for i in range(len(frames))]
     if methods:
         ref = orc.RefEngine(st, threads=threads)
         m = methods[0]
         first = None
-        for i in range(warmup):
-            r, status, out, _ = ref.answer(fl, m)
-            first = out if first is None else first
+        for _ in range(warmup):
+            r, status, out, _ = ref.answer(frames, m)
+            first = out.copy() if first is None else first
         times = []
-        for i in range(steps):
-            t0 = time.perf_counter()
-            r, status, out, _ = ref.answer(fl, m)
-            times.append(time.perf_counter() - t0)
-            first = out if first is None else first
-            assert r == len(fl)
+        while len(times) < steps * min_blocks or sum(times) < min_s:
+            for _ in range(steps):
+                t0 = time.perf_counter()
+                r, status, out, _ = ref.answer(frames, m)
+                times.append(time.perf_counter() - t0)
+                assert r == len(frames)
+        first = out.copy() if first is None else first
         ref.close()
-        kind = "reference"
         name = "reference engine src/amx_kernels.cpp (" + ("AMX" if m == 0 else "AVX-512 VNNI") + ")"
-        qps = len(fl) * len(times) / sum(times)
-        return qps, {"kind": kind, "cores": threads, "engine": name,
-                     "sample": f"{steps} timed batches of {len(fl)} queries after {warmup} warm-up, 1 GiB state",
-                     "median_batch_ms": 1e3 * statistics.median(times)}, first
-    # no AVX-512: the plain-C restatement, on a bounded sample of queries
+        qps = len(frames) * len(times) / sum(times)
+        return qps, {"kind": "reference", "cores": threads, "engine": name,
+                     "sample": f"{len(times)} timed batches of {len(frames)} queries after {warmup} warm-up, {sample}",
+                     "median_batch_ms": 1e3 * statistics.median(times), "timed_s": sum(times)}, first
+    # no AVX-512 on this host: the plain-C restatement, on a bounded sample of queries
     o = orc.Oracle()
-    sub = fl[:8]
+    sub = frames[:8]
     t0 = time.perf_counter()
-    r, status, out = o.answer(st, sub)
+    o.answer(st, sub)
     dt = time.perf_counter() - t0
     return len(sub) / dt, {"kind": "port", "cores": threads, "engine": "oracle/alto_oracle.c",
-                           "sample": f"one batch of {len(sub)} queries"}, None
+                           "sample": f"one batch of {len(sub)} queries, {sample}"}, None
 
 
 def main_reference(a):
+    """The reference arm: the reference's own CPU engine on this arm's workload.  Its state and frames come from the
+    oracle's generators (the same bytes as the engine package's, checked by the CPU tests), so this process never
+    loads the engine library."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    import __graft_entry__ as ge
-    ge.load()
-    from altopir_b200 import service as svc
     from oracle import oracle as orc
-    p, st = reference_state(a, svc)
-    frames = svc.synthetic_requests(p, a.batch, seed=1000)
-    steps, warmup = max(1, a.steps), max(1, a.warmup)
-    # bound the CPU arm to a few minutes: one batch takes ~0.1-0.3 s on 16 AMX cores
-    steps = min(steps, 40)
-    warmup = min(warmup, 3)
-    qps, info, _ = run_reference_cpu(a, svc, orc, st, frames, steps, warmup)
+    o = orc.Oracle()
+    p = orc.Params(a.rows, a.record_bytes)
+    st = orc.State(p, seed=1, oracle=o)
+    frames = o.synthetic_requests(p, a.batch, seed=1000)
+    fl = [frames[i] for i in range(a.batch)]
+    steps, warmup = max(1, a.steps), max(3, a.warmup)
+    qps, info, _ = run_reference_cpu(st, fl, steps, warmup, f"{a.rows * a.record_bytes / 2**30:g} GiB state",
+                                     min_s=MIN_TIMED_S)
     line = {"impl": "reference", "metric": METRIC, "value": qps, "unit": "QPS", "n_gpus": a.gpus, "steps": steps,
             "warmup": warmup, "ms_per_step": 1e3 * a.batch / qps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u8 x u32 limbs -> int32/u64 (exact integer)", "data": "synthetic",
             "config": config_dict(a), "cpu_baseline": dict(info, value=qps, unit="QPS"),
             "e2e": {"value": qps, "unit": "QPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------------------------------------ our arm
+class Measure:
+    """Device-resident, kernel, end-to-end and single-query measurements of one engine at one batch size.  Frames are
+    generated on the device (the bytes of service.synthetic_requests) and copied to pinned host memory for the
+    end-to-end path."""
+
+    def __init__(self, torch, e, p, B, seed, lanes, barrier, world, sampler):
+        from altopir_b200 import service as svc
+        self.torch, self.e, self.p, self.B, self.lanes = torch, e, p, B, lanes
+        self.barrier, self.world, self.sampler = barrier, world, sampler
+        self.rl, self.ql = e.response_len(), e.request_len()
+        self.stride = (7 + self.ql + 255) // 256 * 256
+        # device-resident frames: frame c at slots[c, 7:7 + ql] (the engine's staged layout)
+        self.slots = torch.zeros((B, self.stride), dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()
+        svc.synthetic_requests_device(p, B, seed, self.slots.data_ptr(), self.stride)
+        self.outs = [torch.zeros((B, self.rl), dtype=torch.uint8, device="cuda") for _ in range(lanes)]
+        self.stats = [torch.full((B,), -1, dtype=torch.int32, device="cuda") for _ in range(lanes)]
+        # pinned host frames and outputs for the end-to-end path
+        self.h_req = torch.empty((B, self.ql), dtype=torch.uint8, pin_memory=True)
+        self.h_req.copy_(self.slots[:, 7:7 + self.ql])
+        self.h_out = torch.zeros((B, self.rl), dtype=torch.uint8, pin_memory=True)
+        self.req_ptrs = (ctypes.c_void_p * B)(*[self.h_req.data_ptr() + c * self.ql for c in range(B)])
+        self.lens = (ctypes.c_size_t * B)(*([self.ql] * B))
+        self.out_ptrs = (ctypes.c_void_p * B)(*[self.h_out.data_ptr() + c * self.rl for c in range(B)])
+        self.h_status = np.full(B, -1, dtype=np.int32)
+        self.stream = torch.cuda.ExternalStream(e.stream())
+        torch.cuda.synchronize()  # the buffers above were filled on torch's stream, which the engine's does not wait on
+
+    def frames(self):
+        return self.h_req.numpy()
+
+    def _enqueue(self, i):
+        k = i % self.lanes
+        self.e.enqueue_device(self.slots.data_ptr(), self.stride, self.B, self.outs[k].data_ptr(), self.rl,
+                              self.stats[k].data_ptr())
+
+    def warm(self, warmup):
+        """Untimed: the direct path, alto_answer, then the device path on every lane, each capturing its CUDA graph
+        (left on for device()).  Returns the device time of one direct batch, which sizes the blocks of the larger
+        configurations."""
+        torch, e = self.torch, self.e
+        e.set_graphs(False)
+        e.set_lanes(1)
+        for _ in range(2):
+            e.enqueue_device(self.slots.data_ptr(), self.stride, self.B, self.outs[0].data_ptr(), self.rl,
+                             self.stats[0].data_ptr())
+        e.sync()
+        s, t = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(self.stream)
+        e.enqueue_device(self.slots.data_ptr(), self.stride, self.B, self.outs[0].data_ptr(), self.rl,
+                         self.stats[0].data_ptr())
+        t.record(self.stream)
+        e.sync()
+        est = s.elapsed_time(t)
+        for _ in range(warmup):
+            r = e.answer_raw(self.req_ptrs, self.lens, self.B, self.out_ptrs, self.h_status)
+            if r != self.B:
+                from altopir_b200 import engine as eng
+                raise RuntimeError(f"alto_answer returned {r}: {eng.last_error()}")
+        e.set_graphs(True)
+        e.set_lanes(self.lanes)
+        for i in range(max(warmup, self.lanes)):
+            self._enqueue(i)
+        e.sync()
+        return est
+
+    def _timed(self, body, steps, min_s):
+        torch, e = self.torch, self.e
+        s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        marks = []
+
+        def block():
+            e.sync()
+            torch.cuda.synchronize()
+            t0 = time.time()
+            ms = body(steps, s_ev, e_ev)
+            marks.append((t0, time.time()))
+            self.sampler.mark(*marks[-1])
+            return ms
+
+        times = timed_blocks(block, self.world, self.barrier, min_s=min_s)
+        return times, marks
+
+    def device(self, steps, min_s=MIN_TIMED_S):
+        """value: batches back to back on `lanes` batch contexts with CUDA graph replay; the fences put the start
+        event before every lane's first batch and the end event after every lane's last."""
+        e = self.e
+        e.set_graphs(True)
+        launches = []
+
+        def body(k, s_ev, e_ev):
+            e.set_lanes(self.lanes)  # every block starts at lane 0, so lane j meets the outputs it captured
+            e.fence()
+            s_ev.record(self.stream)
+            e.fence()
+            for i in range(k):
+                self._enqueue(i)
+            e.fence()
+            e_ev.record(self.stream)
+            launches.append(e.last_launches() * k)
+            e.sync()
+            return s_ev.elapsed_time(e_ev)
+
+        times, marks = self._timed(body, steps, min_s)
+        assert all((s == 0).all().item() for s in self.stats)
+        dev_out = self.outs[0].cpu().numpy()
+        assert all(np.array_equal(o.cpu().numpy(), dev_out) for o in self.outs[1:])
+        e.set_graphs(False)
+        e.set_lanes(1)
+        return times, marks, sum(launches), dev_out
+
+    def kernels(self, steps, min_s=MIN_TIMED_S / 2):
+        """Per-kernel durations: the same batches launched directly on one context, every stage bracketed by CUDA
+        events on the engine's stream (graph replays record none)."""
+        e = self.e
+        e.kernel_times(reset=True)
+
+        def body(k, s_ev, e_ev):
+            s_ev.record(self.stream)
+            for _ in range(k):
+                e.enqueue_device(self.slots.data_ptr(), self.stride, self.B, self.outs[0].data_ptr(), self.rl,
+                                 self.stats[0].data_ptr())
+            e_ev.record(self.stream)
+            e.sync()
+            return s_ev.elapsed_time(e_ev)
+
+        self._timed(body, steps, min_s)
+        kms, nb = e.kernel_times(reset=True)
+        return [x / max(nb, 1) for x in kms], nb
+
+    def end_to_end(self, steps, min_s=MIN_TIMED_S):
+        """alto_answer with host buffers: uploads and downloads inside the timed region."""
+        e = self.e
+
+        def body(k, s_ev, e_ev):
+            s_ev.record(self.stream)
+            for _ in range(k):
+                r = e.answer_raw(self.req_ptrs, self.lens, self.B, self.out_ptrs, self.h_status)
+                if r != self.B:
+                    from altopir_b200 import engine as eng
+                    raise RuntimeError(f"alto_answer returned {r}: {eng.last_error()}")
+            e_ev.record(self.stream)
+            self.torch.cuda.synchronize()
+            return s_ev.elapsed_time(e_ev)
+
+        times, marks = self._timed(body, steps, min_s)
+        return times, marks, self.h_out.numpy().copy()
+
+    def plain(self, queries, warmup):
+        """The plain path: one query per batch, each waited for.  As a single-query server does, every frame is
+        staged into one fixed slot (a device-to-device copy inside the timed region) and the engine replays the
+        launch sequence it captured for that slot as a CUDA graph."""
+        torch, e = self.torch, self.e
+        one = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stage = torch.zeros((1, self.stride), dtype=torch.uint8, device="cuda")
+        stage_out = torch.zeros((1, self.rl), dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()
+        e.set_graphs(True)
+
+        def go(c):
+            with torch.cuda.stream(self.stream):
+                stage.copy_(self.slots[c:c + 1], non_blocking=True)
+            e.enqueue_device(stage.data_ptr(), self.stride, 1, stage_out.data_ptr(), self.rl, None)
+
+        for i in range(warmup):  # untimed: kernel loading and the graph's capture
+            go(i % self.B)
+        e.sync()
+        check = bool(torch.equal(stage_out[0], self.outs[0][(warmup - 1) % self.B]))
+        self.barrier()
+        lat = []
+        t0 = time.time()
+        for i in range(queries):
+            one[0].record(self.stream)
+            go(i % self.B)
+            one[1].record(self.stream)
+            e.sync()
+            lat.append(one[0].elapsed_time(one[1]))
+        self.sampler.mark(t0, time.time())
+        e.set_graphs(False)
+        total = max_over_ranks(sum(lat), self.world)
+        ls = sorted(lat)
+        return {"qps": self.world * queries / (total * 1e-3), "queries": queries, "p50_ms": ls[len(ls) // 2],
+                "p99_ms": ls[min(len(ls) - 1, int(len(ls) * 0.99))],
+                "api": "alto_enqueue_device, one frame staged into a fixed slot, CUDA graph replay"}, check
+
+    def close(self):
+        del self.slots, self.outs, self.stats, self.h_req, self.h_out
+        self.torch.cuda.empty_cache()
+
+
+def summarize(m, p, B, steps, world, dev, kern, e2e, plain, peaks, peak_src, traffic=None):
+    """The JSON fields of one configuration from its measurements."""
+    (dtimes, dmarks, launches, dev_out), (kms, nb), (etimes, emarks, host_out) = dev, kern, e2e
+    nblocks, eblocks = len(dtimes), len(etimes)
+    value = job_qps(world, B, steps * nblocks, sum(dtimes))
+    e2e_qps = job_qps(world, B, steps * eblocks, sum(etimes))
+    alg = algorithmic(p.rows, p.record_bytes, B, p.count)
+    avg = {"scan_gemm": kms[2], "pack_gemm": kms[3]}
+    dom = max(avg, key=avg.get)
+    kernels = {}
+    for k, ms in avg.items():
+        kernels[k] = {"avg_ms": ms, "tops": alg[k]["ops"] / (ms * 1e-3) / 1e12,
+                      "gbs": alg[k]["bytes"] / (ms * 1e-3) / 1e9}
+    kernels.update({"validate": {"avg_ms": kms[0]}, "limb_split": {"avg_ms": kms[1]}, "tail": {"avg_ms": kms[4]},
+                    "batches_timed": nb})
+    bpq = {"value": value, "unit": "QPS", "ms_per_step": sum(dtimes) / (steps * nblocks)}
+    return {
+        "value": value, "ms_per_step": bpq["ms_per_step"], "steps": steps, "blocks": nblocks,
+        "timed_region_s": sum(dtimes) / 1e3,
+        "block_ms_per_step": {"min": min(dtimes) / steps, "median": statistics.median(dtimes) / steps,
+                              "max": max(dtimes) / steps},
+        "e2e": {"value": e2e_qps, "unit": "QPS", "h2d_bytes_per_step": B * m.ql, "d2h_bytes_per_step": B * m.rl + 4 * B,
+                "ms_per_step": sum(etimes) / (steps * eblocks), "blocks": eblocks,
+                "timed_region_s": sum(etimes) / 1e3, "api": "alto_answer (pinned host frames and outputs)"},
+        "gpu_launches": launches,
+        "roofline": roofline_of(dom, alg[dom], avg[dom], peaks, peak_src, traffic),
+        "kernels": kernels,
+        "plain_per_query": dict(plain[0], batched_over_plain=value / plain[0]["qps"]),
+        "byte_exact": {"device_vs_host_path": bool(np.array_equal(dev_out, host_out)), "plain_vs_batched": plain[1]},
+    }
+
+
+def engine_for(svc, eng, p, host_db):
+    """An engine over the seeded synthetic state; without host_db the database is generated on the device."""
+    st = svc.SyntheticState.make(p, seed=1, keep_values=host_db, host_db=host_db)
+    e = eng.Engine.from_state(st, threads=svc.threads(), tile=False)
+    st.ub = None
+    return st, e
+
+
+def main_ours(a):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    import __graft_entry__ as ge
+    ge.load()
+    from altopir_b200 import engine as eng, service as svc
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    eng.init()
+    K, W = max(1, a.steps), max(3, a.warmup)
+    lanes = max(1, min(4, a.lanes))
+    peaks, peak_src = measured_peaks()
+    int8_tops = int8_cublas_tops(torch) if rank == 0 else None
+    sampler = ClockSampler()
+    if rank == 0:
+        sampler.start()
+
+    # ---- the headline configuration
+    p = svc.params(a.rows, a.record_bytes)
+    want_cpu = rank == 0 and world == 1 and not a.no_cpu_baseline
+    st, e = engine_for(svc, eng, p, host_db=want_cpu)
+    m = Measure(torch, e, p, a.batch, 1000 + rank, lanes, barrier, world, sampler)
+    m.warm(W)
+    dev = m.device(K)
+    kern = m.kernels(K)
+    e2e = m.end_to_end(K)
+    plain = m.plain(a.plain_queries, W)
+    head_clocks = sampler.summary()
+    res = summarize(m, p, a.batch, K, world, dev, kern, e2e, plain, peaks, peak_src,
+                    traffic_from_profile("scan_gemm" if kern[0][2] >= kern[0][3] else "pack_gemm", a.rows,
+                                         a.record_bytes, a.batch))
+    frames = m.frames().copy() if want_cpu else None
+    m.close()
+    e.close()
+
+    cpu_baseline, exact_vs_ref = None, None
+    if want_cpu:
+        qps_cpu, info, ref_out = run_reference_cpu(st, [frames[i] for i in range(a.batch)], steps=5, warmup=1,
+                                                   sample=f"{a.rows * a.record_bytes / 2**30:g} GiB state")
+        cpu_baseline = dict(info, value=qps_cpu, unit="QPS")
+        if ref_out is not None:
+            exact_vs_ref = bool(np.array_equal(ref_out, dev[3]))
+    st = None
+
+    # ---- the larger databases (rank 0 of a one-GPU run): blocks of up to K steps, about 0.2 s each
+    configs = []
+    if world == 1 and not a.no_configs:
+        for rows, batches, plain_q in SUB_CONFIGS:
+            pp = svc.params(rows, a.record_bytes)
+            _, e = engine_for(svc, eng, pp, host_db=False)
+            for B in batches:
+                mark0 = len(sampler.marks)
+                m = Measure(torch, e, pp, B, 2000, lanes, barrier, world, sampler)
+                est = m.warm(W)
+                k = int(max(1, min(K, math.ceil(200.0 / max(est, 1e-3)))))
+                d = m.device(k)
+                kk = m.kernels(k, min_s=0.3)
+                ee = m.end_to_end(k)
+                pl = m.plain(plain_q, 3)
+                r = summarize(m, pp, B, k, world, d, kk, ee, pl, peaks, peak_src)
+                pub = PUBLISHED_QPS.get(rows)
+                r.update({"config": config_dict(a, rows, B), "clocks": sampler.summary(sampler.marks[mark0:]),
+                          "vs_baseline": r["value"] / pub[0] if pub else None,
+                          "vs_baseline_ref": f"{pub[0]} QPS, {pub[1]}" if pub else None})
+                configs.append(r)
+                print(f"config {rows} records, B = {B}: {r['value']:.0f} QPS device, {r['e2e']['value']:.0f} e2e, "
+                      f"frac {r['roofline']['frac']:.3f}", file=sys.stderr, flush=True)
+                m.close()
+            e.close()
+            torch.cuda.empty_cache()
+    sampler.stop()
+
+    if rank == 0:
+        pub = PUBLISHED_QPS.get(a.rows) if (a.batch == 128 and a.record_bytes == 32768) else None
+        clocks = dict(head_clocks)
+        if clocks.get("sm_mhz"):
+            clocks["ms_per_step_x_sm_mhz"] = res["ms_per_step"] * clocks["sm_mhz"]
+        line = {
+            "metric": METRIC, "value": res["value"], "unit": "QPS", "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": res["value"] / pub[0] if pub else None,
+            "vs_baseline_ref": f"{pub[0]} QPS, {pub[1]}, 16-core Xeon Silver 4514Y (AMX)" if pub else None,
+            "dtype": "u8 x u8 limbs -> int32 (tcgen05 kind::i8), exact", "data": "synthetic",
+            "config": config_dict(a), "parallelism": f"replicas{world}",
+            "blocks": res["blocks"], "timed_region_s": res["timed_region_s"],
+            "block_ms_per_step": res["block_ms_per_step"],
+            "e2e": res["e2e"], "gpu_launches": res["gpu_launches"],
+            "api": f"alto_enqueue_device (frames resident in HBM) rotating through {lanes} batch context(s) "
+                   "(alto_engine_set_lanes; consecutive batches overlap on the device), launch sequence replayed as "
+                   "a CUDA graph; kernels and roofline from a second pass of the same batches launched directly on "
+                   "one context",
+            "roofline": dict(res["roofline"], int8_cublaslt_tops=int8_tops),
+            "kernels": res["kernels"], "cpu_baseline": cpu_baseline, "clocks": clocks,
+            "plain_per_query": res["plain_per_query"],
+            "byte_exact": dict(res["byte_exact"], vs_reference_engine=exact_vs_ref),
+            "configs": configs,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
     return 0
 
 
@@ -294,228 +709,6 @@ def main_serve(a):
             "rates": rows}
     print(json.dumps(line))
     e.close()
-    return 0
-
-
-# ------------------------------------------------------------------------------------------------ our arm
-def main_ours(a):
-    import torch
-    import torch.distributed as dist
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
-    import __graft_entry__ as ge
-    ge.load()
-    from altopir_b200 import engine as eng, service as svc
-
-    eng.init()
-    p = svc.params(a.rows, a.record_bytes)
-    want_cpu = rank == 0 and world == 1 and not a.no_cpu_baseline
-    st = svc.SyntheticState.make(p, seed=1, keep_values=want_cpu)
-    # the engine reads the column-order database; skip the host tiled copy of very large databases
-    e = eng.Engine.from_state(st, threads=svc.threads(), tile=a.rows * a.record_bytes <= (8 << 30))
-    if not want_cpu:
-        st.ub = None
-    B, rl, ql = a.batch, e.response_len(), e.request_len()
-    frames = svc.synthetic_requests(p, B, seed=1000 + rank)
-
-    # device-resident frames: frame c at slots[c, 7:7 + ql] (the engine's staged layout)
-    stride = (7 + ql + 255) // 256 * 256
-    slots = torch.zeros((B, stride), dtype=torch.uint8, device="cuda")
-    slots[:, 7:7 + ql] = torch.from_numpy(frames).cuda()
-    d_out = torch.zeros((B, rl), dtype=torch.uint8, device="cuda")
-    d_status = torch.full((B,), -1, dtype=torch.int32, device="cuda")
-    # pinned host frames and outputs for the end-to-end path
-    h_req = torch.from_numpy(frames).pin_memory()
-    h_out = torch.zeros((B, rl), dtype=torch.uint8).pin_memory()
-    req_ptrs = (ctypes.c_void_p * B)(*[h_req.data_ptr() + c * ql for c in range(B)])
-    lens = (ctypes.c_size_t * B)(*([ql] * B))
-    out_ptrs = (ctypes.c_void_p * B)(*[h_out.data_ptr() + c * rl for c in range(B)])
-    h_status = np.full(B, -1, dtype=np.int32)
-    stream = torch.cuda.ExternalStream(e.stream())
-    torch.cuda.synchronize()  # the buffers above were filled on torch's stream, which the engine's does not wait on
-
-    peaks, peak_src = measured_peaks()
-    int8_tops = int8_cublas_tops(torch) if rank == 0 else None
-    sampler = ClockSampler()
-    if rank == 0:
-        sampler.start()
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    # ---- warm-up (both paths); the device path rotates through `lanes` batch contexts, lane k writing outputs k, and
-    # replays its launch sequence as a CUDA graph, captured on each lane's first warm-up batch
-    lanes = max(1, min(4, a.lanes))
-    outs = [d_out] + [torch.zeros_like(d_out) for _ in range(lanes - 1)]
-    stats = [d_status] + [torch.full_like(d_status, -1) for _ in range(lanes - 1)]
-    torch.cuda.synchronize()
-    e.set_graphs(True)
-    e.set_lanes(lanes)
-    for i in range(max(3, a.warmup, lanes)):
-        k = i % lanes
-        e.enqueue_device(slots.data_ptr(), stride, B, outs[k].data_ptr(), rl, stats[k].data_ptr())
-    e.sync()
-    e.set_lanes(lanes)  # the timed batches start again at lane 0, so lane k meets the outputs it captured
-    for _ in range(max(3, a.warmup)):
-        r = e.answer_raw(req_ptrs, lens, B, out_ptrs, h_status)
-        assert r == B, (r, eng.last_error())
-
-    # ---- value: device-resident batches back to back
-    e.kernel_times(reset=True)
-    barrier()
-    torch.cuda.synchronize()
-    e.sync()
-    s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    t0 = time.time()
-    # the fences put the start event before every lane's first batch and the end event after every lane's last
-    e.fence()
-    s_ev.record(stream)
-    e.fence()
-    for i in range(a.steps):
-        k = i % lanes
-        e.enqueue_device(slots.data_ptr(), stride, B, outs[k].data_ptr(), rl, stats[k].data_ptr())
-    e.fence()
-    e_ev.record(stream)
-    e.sync()
-    torch.cuda.synchronize()
-    t1 = time.time()
-    sampler.mark(t0, t1)
-    value_ms = max_over_ranks(s_ev.elapsed_time(e_ev), world)
-    launches = e.last_launches() * a.steps
-    assert all((s == 0).all().item() for s in stats)
-    dev_out = d_out.cpu().numpy()
-    assert all(np.array_equal(o.cpu().numpy(), dev_out) for o in outs[1:])
-    e.set_graphs(False)
-    e.set_lanes(1)
-
-    # ---- per-kernel durations (the roofline's): the same batches again, launched directly so that every stage is
-    # bracketed by CUDA events on the engine's stream (graph replays record none)
-    e.kernel_times(reset=True)
-    t0 = time.time()
-    for _ in range(a.steps):
-        e.enqueue_device(slots.data_ptr(), stride, B, d_out.data_ptr(), rl, d_status.data_ptr())
-    e.sync()
-    sampler.mark(t0, time.time())
-    kms, nb = e.kernel_times(reset=True)
-    assert nb == a.steps and np.array_equal(d_out.cpu().numpy(), dev_out)
-
-    # ---- e2e: the C ABI with host buffers (uploads and downloads inside the timed region)
-    barrier()
-    torch.cuda.synchronize()
-    s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    t0 = time.time()
-    s2.record(stream)
-    for _ in range(a.steps):
-        r = e.answer_raw(req_ptrs, lens, B, out_ptrs, h_status)
-        if r != B:
-            raise RuntimeError(f"alto_answer returned {r}: {eng.last_error()}")
-    e2.record(stream)
-    torch.cuda.synchronize()
-    t1 = time.time()
-    sampler.mark(t0, t1)
-    e2e_ms = max_over_ranks(s2.elapsed_time(e2), world)
-    host_out = h_out.numpy().copy()
-    e.kernel_times(reset=True)
-
-    # ---- the plain path: one query per batch, each waited for.  As a single-query server does, every frame is
-    # staged into one fixed slot (a device-to-device copy inside the timed region) and the engine replays the launch
-    # sequence it captured for that slot as a CUDA graph.
-    lat = []
-    one = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    stage = torch.zeros((1, stride), dtype=torch.uint8, device="cuda")
-    stage_out = torch.zeros((1, rl), dtype=torch.uint8, device="cuda")
-    e.set_graphs(True)
-
-    def plain(c):
-        with torch.cuda.stream(stream):
-            stage.copy_(slots[c:c + 1], non_blocking=True)
-        e.enqueue_device(stage.data_ptr(), stride, 1, stage_out.data_ptr(), rl, None)
-
-    for i in range(max(3, a.warmup)):  # untimed: kernel loading and the graph's capture
-        plain(i % B)
-    e.sync()
-    plain_check = bool(torch.equal(stage_out[0], d_out[(max(3, a.warmup) - 1) % B]))
-    barrier()
-    for i in range(a.plain_queries):
-        one[0].record(stream)
-        plain(i % B)
-        one[1].record(stream)
-        e.sync()
-        lat.append(one[0].elapsed_time(one[1]))
-    e.set_graphs(False)
-    plain_total = max_over_ranks(sum(lat), world)
-    sampler.stop()
-
-    byte_exact_paths = bool(np.array_equal(dev_out, host_out))
-
-    # ---- roofline of the dominant kernel (CUDA events on the engine stream over the timed region)
-    alg = algorithmic(p.rows, p.record_bytes, B, p.count)
-    avg = {"scan_gemm": kms[2] / max(nb, 1), "pack_gemm": kms[3] / max(nb, 1)}
-    dom = max(avg, key=avg.get)
-    int8_peak = 2.0 * peaks["bf16_tflops"]
-    kernels = {}
-    for k, ms in avg.items():
-        kernels[k] = {"avg_ms": ms, "tops": alg[k]["ops"] / (ms * 1e-3) / 1e12,
-                      "gbs": alg[k]["bytes"] / (ms * 1e-3) / 1e9}
-    kernels["validate"] = {"avg_ms": kms[0] / max(nb, 1)}
-    kernels["limb_split"] = {"avg_ms": kms[1] / max(nb, 1)}
-    kernels["tail"] = {"avg_ms": kms[4] / max(nb, 1)}
-    traffic = traffic_from_profile(dom, a.rows, a.record_bytes, B)
-    roofline = {"kernel": dom, "bound": "tensor", "achieved": kernels[dom]["tops"], "peak": int8_peak,
-                "unit": "TFLOP/s", "frac": kernels[dom]["tops"] / int8_peak, "traffic": traffic,
-                "peak_source": f"2 x {peak_src} dense bf16 ({peaks['bf16_tflops']} TF/s; B200 int8 dense rate = 2x "
-                               f"bf16); int8 ops counted as 2 per multiply-add",
-                "hbm_view": {"achieved_gbs": kernels[dom]["gbs"], "peak_gbs": peaks["hbm_gbs"],
-                             "frac": kernels[dom]["gbs"] / peaks["hbm_gbs"]},
-                "int8_cublaslt_tops": int8_tops, "algorithmic_bytes": alg[dom]["bytes"],
-                "algorithmic_ops": alg[dom]["ops"]}
-
-    cpu_baseline = None
-    exact_vs_ref = None
-    if want_cpu:
-        from oracle import oracle as orc
-        del e
-        qps_cpu, info, ref_out = run_reference_cpu(a, svc, orc, st, frames, steps=5, warmup=1)
-        cpu_baseline = dict(info, value=qps_cpu, unit="QPS")
-        if ref_out is not None:
-            exact_vs_ref = bool(np.array_equal(ref_out, dev_out))
-
-    if rank == 0:
-        value = job_qps(world, B, a.steps, value_ms)
-        e2e = job_qps(world, B, a.steps, e2e_ms)
-        lat_sorted = sorted(lat)
-        line = {
-            "metric": METRIC, "value": value, "unit": "QPS", "n_gpus": world, "steps": a.steps,
-            "warmup": max(3, a.warmup), "ms_per_step": value_ms / a.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u8 x u8 limbs -> int32 (tcgen05 kind::i8), exact",
-            "data": "synthetic", "config": dict(config_dict(a), parallelism=f"replicas{world}"),
-            "e2e": {"value": e2e, "unit": "QPS", "h2d_bytes_per_step": B * ql, "d2h_bytes_per_step": B * rl + 4 * B,
-                    "ms_per_step": e2e_ms / a.steps, "api": "alto_answer (pinned host frames and outputs)"},
-            "gpu_launches": launches,
-            "api": f"alto_enqueue_device (frames resident in HBM) rotating through {lanes} batch context(s) "
-                   "(alto_engine_set_lanes; consecutive batches overlap on the device), launch sequence replayed as "
-                   "a CUDA graph; kernels and roofline from a second pass of the same batches launched directly on "
-                   "one context",
-            "roofline": roofline,
-            "kernels": kernels,
-            "cpu_baseline": cpu_baseline,
-            "clocks": sampler.summary(),
-            "plain_per_query": {"qps": world * a.plain_queries / (plain_total * 1e-3),
-                                "p50_ms": lat_sorted[len(lat) // 2], "p99_ms": lat_sorted[int(len(lat) * 0.99)],
-                                "batched_over_plain": value / (world * a.plain_queries / (plain_total * 1e-3)),
-                                "api": "alto_enqueue_device, one frame staged into a fixed slot, CUDA graph replay"},
-            "byte_exact": {"device_vs_host_path": byte_exact_paths, "vs_reference_engine": exact_vs_ref,
-                           "plain_vs_batched": plain_check},
-        }
-        print(json.dumps(line))
-    if world > 1:
-        dist.destroy_process_group()
     return 0
 
 

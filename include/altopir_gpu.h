@@ -53,8 +53,10 @@ void sw_pack_build(int8_t *ub, const uint64_t *const *bold_t, const uint64_t *co
  * db_tiled must be non-NULL but is not read.  The database, the packing matrix `ub` (layout of sw_pack_build),
  * the row-0 prefixes (cols / n buffers of part_len bytes), bold_t_hat (`that`, cols / n arrays of tg * n words,
  * reduced mod q) and the low 32 bits of inv_table[0..n) are copied into device memory, so the caller may free all
- * of them once this returns.  Returns NULL when the configuration is unsupported or the device lacks memory
- * (alto_last_error() says which). */
+ * of them once this returns.  `ub` must have been written by this library's sw_pack_build (or alto_pack_encode):
+ * a buffer in the reference's AMX layout (sw_ubt, -128-biased tile order), for example one cached from a build of
+ * src/amx_kernels.cpp, has the same size but other bytes, and the engine would answer with wrong responses.
+ * Returns NULL when the configuration is unsupported or the device lacks memory (alto_last_error() says which). */
 void *alto_engine_new(const uint8_t *db_col, const uint8_t *db_tiled, size_t ld, size_t rows, size_t cols,
                       const int8_t *ub, size_t n, size_t tg, const uint8_t *const *prefix, size_t part_len,
                       size_t row1_off, uint64_t q1, int q1_bits, const uint64_t *const *that,
@@ -171,8 +173,10 @@ int alto_kernel_times(void *engine, double *ms, long long *batches, int reset);
  * cudaMalloc's device-wide synchronisation.  Frames and outputs are laid out as for alto_answer_device; statuses go
  * to the device array d_status[b].  The per-batch scratch (statuses, byte limbs, scan sums, pack results) lives in
  * a fixed 16 MiB array inside this library, which every GPU that loads the library holds until the process exits;
- * a batch whose scratch would exceed it is rejected with -1 and a message in alto_last_error() (at 32768 records of
- * 32 KB that is about 36 frames).  The first call on a device looks up the array's device address (set-up done
+ * a batch whose scratch would exceed it is rejected with -1 and a message in alto_last_error().  A batch of b frames
+ * needs, with every term rounded up to 256 bytes and b4 = b rounded up to 4, R = rows (rows rounded up to 32768 above
+ * 32768 records), cols = record bytes, K = tg * n:  4 b + 4 b4 R + 4 b4 K + 2 * 4 b cols <= 16 MiB.  At 32768 records
+ * of 32 KB (K = 8192) that allows 38 frames.  The first call on a device looks up the array's device address (set-up done
  * once per device), so that first call should come before any stream capture.  All calls share the array: calls
  * whose work overlaps on the GPU race, even on different engines of the same device.  Returns 0 once the batch has
  * completed, -1, -3 or -4 as alto_answer. */
@@ -239,9 +243,18 @@ int alto_engine_load_file(void *engine, const char *path, size_t num_real_rows);
  * alto_fill_bytes: dst[i] = uniform bytes from the same counter construction.
  * alto_synthetic_request: a well-formed frame of alto_request_len bytes for a seeded client: y, z uniform in
  *   [0, 4294955009), query words uniform over u32 (the distribution of rounded RLWE query words).
- * alto_pack_encode: packing-matrix values U[col * K + k] (< 2^32) into the layout of sw_pack_build. */
+ * alto_pack_encode: packing-matrix values U[col * K + k] (< 2^32) into the layout of sw_pack_build.
+ * alto_engine_fill_synthetic: fills the whole database of an engine with the synthetic records on the device (the
+ *   bytes alto_synthetic_db_col gives), so large databases need no host copy; waits for the engine's batches first.
+ *   0, -1 (NULL engine) or -4.
+ * alto_synthetic_requests_device: b frames of alto_synthetic_request (clients first_client ..), frame c written to
+ *   d_slots + c * stride + lead in device memory; needs (lead + 9) % 4 == 0, stride % 4 == 0, d_slots 4-byte aligned,
+ *   stride >= lead + 9 + 4 * (2 * tg_n + rows), b <= 65535.  0, -1 (bad arguments) or -4. */
 void alto_synthetic_db_col(uint8_t *db, size_t ld, size_t rows, size_t col0, size_t ncols, int threads);
 int alto_synthetic_db_col_device(uint8_t *d_db, size_t ld, size_t rows, size_t col0, size_t ncols);
+int alto_engine_fill_synthetic(void *engine);
+int alto_synthetic_requests_device(uint8_t *d_slots, size_t stride, size_t lead, size_t b, size_t rows, size_t tg_n,
+                                   uint64_t seed, uint64_t first_client);
 void alto_fill_uniform_u32(uint32_t *dst, size_t count, uint64_t bound, uint64_t seed, int threads);
 void alto_fill_uniform_u64(uint64_t *dst, size_t count, uint64_t bound, uint64_t seed, int threads);
 void alto_fill_bytes(uint8_t *dst, size_t count, uint64_t seed, int threads);

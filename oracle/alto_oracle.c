@@ -73,6 +73,44 @@ void orc_synthetic_db_col(uint8_t *db, size_t ld, size_t rows, size_t col0, size
         for (size_t r = 0; r < rows; r++) db[c * ld + r] = orc_record_byte(r, col0 + c);
 }
 
+/* ------------------------------------------------------------------ seeded benchmark inputs
+ * The seeded engine state and request frames that the tests and the benchmark give to both engines.  The reference
+ * builds its state with spiral-rs and its clients draw secrets from entropy, so these inputs are this project's own
+ * definition, not a reference algorithm: value i of a stream with counter `seed` is the splitmix64 finaliser of
+ * seed + (i + 1) * gamma, mapped to [0, bound) by a multiply-high of its top 32 bits.  The engine library carries the
+ * same generators (alto_fill_*, alto_synthetic_request); this copy lets the benchmark's reference arm build its
+ * workload without loading the engine library, and the CPU tests check that the two copies agree byte for byte. */
+static inline uint64_t orc_stream_at(uint64_t seed, uint64_t i) { return orc_finalise(seed + (i + 1) * ORC_GAMMA); }
+static inline uint64_t orc_bounded(uint64_t x, uint64_t bound) { return ((x >> 32) * bound) >> 32; }
+
+void orc_fill_uniform_u32(uint32_t *dst, size_t count, uint64_t bound, uint64_t seed) {
+    #pragma omp parallel for schedule(static)
+    for (size_t i = 0; i < count; i++) dst[i] = (uint32_t)orc_bounded(orc_stream_at(seed, i), bound);
+}
+
+void orc_fill_uniform_u64(uint64_t *dst, size_t count, uint64_t bound, uint64_t seed) {
+    #pragma omp parallel for schedule(static)
+    for (size_t i = 0; i < count; i++) dst[i] = orc_bounded(orc_stream_at(seed, i), bound);
+}
+
+void orc_fill_bytes(uint8_t *dst, size_t count, uint64_t seed) {
+    #pragma omp parallel for schedule(static)
+    for (size_t i = 0; i < count; i++) dst[i] = (uint8_t)(orc_stream_at(seed, i) >> 56);
+}
+
+/* One well-formed frame of client `client`: [0][u32 tg_n][u32 tg_n][y, z: 2 tg_n words < Q][rows query words], the
+ * frame layout of src/service.rs:178-198; stream counter seed ^ ORC_ROW_MUL * (client + 1). */
+void orc_synthetic_request(uint8_t *frame, size_t rows, size_t tg_n, uint64_t seed, uint64_t client) {
+    const uint64_t s = seed ^ (ORC_ROW_MUL * (client + 1));
+    frame[0] = 0;
+    for (int b = 0; b < 4; b++) frame[1 + b] = frame[5 + b] = (uint8_t)(tg_n >> (8 * b));
+    for (size_t i = 0; i < 2 * tg_n + rows; i++) {
+        const uint64_t x = orc_stream_at(s, i);
+        const uint32_t v = i < 2 * tg_n ? (uint32_t)orc_bounded(x, ORC_Q) : (uint32_t)(x >> 32);
+        for (int b = 0; b < 4; b++) frame[9 + 4 * i + b] = (uint8_t)(v >> (8 * b));
+    }
+}
+
 /* ------------------------------------------------------------------ request validation (amx_kernels.cpp:572-580) */
 
 /* Status of one request frame, as alto_answer assigns it (amx_kernels.cpp:572-580) and as decode_request rejects it

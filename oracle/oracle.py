@@ -16,10 +16,19 @@ REF_SO = os.path.join(HERE, "_ref", "libalto_ref.so")
 Q = 4294955009
 
 
+# Where the reference tree is mounted when this repository is built (override with ALTO_REFERENCE_DIR); the GPU
+# machines have no reference tree and use the _ref/ library built here.
+REFERENCE_DIR = os.environ.get("ALTO_REFERENCE_DIR", "/root/reference")
+
+
 def build():
-    """Compiles liboracle.so (and _ref/ when the reference tree is present) with oracle/Makefile."""
+    """Compiles liboracle.so (and _ref/ from the reference's own source when the reference tree is present) with
+    oracle/Makefile."""
     import subprocess
-    r = subprocess.run(["make", "-s", "-C", HERE], capture_output=True, text=True)
+    args = ["make", "-s", "-C", HERE]
+    if os.path.isdir(REFERENCE_DIR):
+        args.append(f"REFERENCE_DIR={REFERENCE_DIR}")
+    r = subprocess.run(args, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)
 
@@ -95,6 +104,10 @@ class Oracle:
             ("orc_answer", I, [c.POINTER(_OrcState), c.POINTER(P), c.POINTER(S), S, c.POINTER(P), c.POINTER(I)]),
             ("orc_pack_build", None, [P, c.POINTER(P), c.POINTER(P), P, P, S, S, S, S]),
             ("orc_answer_parts", I, [c.POINTER(_OrcState), c.POINTER(P), c.POINTER(S), S, c.POINTER(P)]),
+            ("orc_fill_uniform_u32", None, [P, S, U64, U64]),
+            ("orc_fill_uniform_u64", None, [P, S, U64, U64]),
+            ("orc_fill_bytes", None, [P, S, U64]),
+            ("orc_synthetic_request", None, [P, S, S, U64, U64]),
         ]:
             f = getattr(L, name)
             f.restype, f.argtypes = res, args
@@ -191,6 +204,76 @@ class Oracle:
 
     def scan_acc(self, dbcol, qwords_u8):
         return self.L.orc_scan_acc(_p(dbcol), _p(qwords_u8), dbcol.size)
+
+
+    def fill_uniform_u32(self, count, bound, seed):
+        out = np.empty(count, dtype=np.uint32)
+        self.L.orc_fill_uniform_u32(_p(out), count, bound, seed)
+        return out
+
+    def fill_uniform_u64(self, count, bound, seed):
+        out = np.empty(count, dtype=np.uint64)
+        self.L.orc_fill_uniform_u64(_p(out), count, bound, seed)
+        return out
+
+    def fill_bytes(self, count, seed):
+        out = np.empty(count, dtype=np.uint8)
+        self.L.orc_fill_bytes(_p(out), count, seed)
+        return out
+
+    def synthetic_requests(self, p, b, seed, first_client=0):
+        """b frames of the seeded synthetic clients first_client .. as a (b, request_len) uint8 array."""
+        out = np.empty((b, 9 + 4 * (2 * p.count + p.rows)), dtype=np.uint8)
+        for c in range(b):
+            self.L.orc_synthetic_request(_p(out[c]), p.rows, p.count, seed, first_client + c)
+        return out
+
+
+# --------------------------------------------------------------------------------------------- seeded state
+class Params:
+    """The scheme parameters of the answer path (src/service.rs:19-41, params.rs:97-125): n = 2048, tg = 4, row 0
+    switched to 18 bits and row 1 to 10 bits, so a response part is 7168 bytes."""
+
+    def __init__(self, rows, record_bytes, n=2048, tg=4, q1_bits=10, q2_bits=18):
+        self.rows, self.record_bytes, self.n, self.tg = rows, record_bytes, n, tg
+        self.q1_bits, self.row1_off = q1_bits, q2_bits * n
+        self.instances, self.count = record_bytes // n, tg * n
+        self.row0_bytes = (q2_bits * n + 7) // 8
+        self.part_len = ((q2_bits * n + q1_bits * n + 63) // 64 * 64 + 7) // 8
+
+
+def inverse_ntt_table(n):
+    """Inverse powers of a primitive 2n-th root of unity mod Q in bit-reversed order, the table shape the engines
+    index as [h + i] for block i of the stage with h blocks."""
+    logn = n.bit_length() - 1
+    for g in range(2, 1000):
+        psi = pow(g, (Q - 1) // (2 * n), Q)
+        if pow(psi, n, Q) == Q - 1:
+            break
+    inv = pow(psi, Q - 2, Q)
+    rev = [int(format(i, f"0{logn}b")[::-1], 2) if logn else 0 for i in range(n)]
+    return np.array([pow(inv, r, Q) for r in rev], dtype=np.uint64)
+
+
+class State:
+    """Seeded engine state with the shapes of the reference's (src/service.rs:127-170): the synthetic column-order
+    database, packing-matrix values U uniform in [0, Q), bold_t_hat uniform in [0, Q), row-0 prefixes (random bytes
+    in the row-0 bits, zero after them) and an inverse-NTT table.  Built with this oracle's generators only; for the
+    same (rows, record_bytes, seed) it holds the bytes that the engine package's SyntheticState.make produces."""
+
+    def __init__(self, p, seed=1, oracle=None):
+        o = oracle or Oracle()
+        self.p, self.seed = p, seed
+        self.db_col = o.synthetic_db_col(p.rows, 0, p.record_bytes)
+        base = seed * 0x1000193
+        self.U = o.fill_uniform_u32(p.record_bytes * p.count, Q, base + 1).reshape(p.record_bytes, p.count)
+        self.that = [o.fill_uniform_u64(p.count, Q, base + 2 + k) for k in range(p.instances)]
+        self.prefixes = []
+        for k in range(p.instances):
+            pre = o.fill_bytes(p.part_len, base + 100 + k)
+            pre[p.row0_bytes:] = 0
+            self.prefixes.append(pre)
+        self.inv_table = inverse_ntt_table(p.n)
 
 
 # --------------------------------------------------------------------------------------------- reference engine

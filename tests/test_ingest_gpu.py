@@ -67,3 +67,30 @@ def test_record_file_shorter_than_the_database_reads_as_zero_padded(gpu, oracle,
     with pytest.raises(eng.EngineError):
         e.load_file(path, real + 128)  # the file is short
     e.close()
+
+
+def test_database_and_frames_generated_on_the_device_equal_the_host_generators(gpu, svc, eng, oracle):
+    """alto_engine_fill_synthetic writes the synthetic records into the tiles (including a record count off the
+    128-record grid, whose padding records stay zero) and alto_synthetic_requests_device writes the frames of
+    alto_synthetic_request: the engine answers as one built from the host's column-order database."""
+    import torch
+    for rows, rb in ((4096, 8192), (8256, 4096)):
+        p = svc.Params(rows, rb)
+        st = svc.SyntheticState.make(p, seed=95)
+        dev = svc.SyntheticState.make(p, seed=95, host_db=False)
+        assert dev.db_col is None
+        ql = svc.request_len(p)
+        stride = (7 + ql + 255) // 256 * 256
+        slots = torch.zeros((5, stride), dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()
+        svc.synthetic_requests_device(p, 5, 96, slots.data_ptr(), stride, first_client=3)
+        frames = slots[:, 7:7 + ql].cpu().numpy()
+        assert np.array_equal(frames, svc.synthetic_requests(p, 5, seed=96, first_client=3))
+        full = eng.Engine.from_state(st)
+        want = _answer(full, frames)
+        full.close()
+        e = eng.Engine.from_state(dev)
+        assert np.array_equal(_answer(e, frames), want)
+        e.close()
+        r, _, ref = oracle.answer(st, [frames[i] for i in range(5)])
+        assert r == 5 and np.array_equal(ref, want)

@@ -160,3 +160,22 @@ def test_pack_build_at_the_scheme_shape_matches_oracle(oracle, svc, eng):
     planes = ub.view(np.uint8).reshape(rho * n, 4, tg * n).astype(np.uint32)
     mine = planes[:, 0] | (planes[:, 1] << 8) | (planes[:, 2] << 16) | (planes[:, 3] << 24)
     assert np.array_equal(mine, oracle.pack_build(bt, btb, tables, gen_pows, it, tg, n))
+
+
+def test_oracle_state_and_frames_equal_the_engine_generators(oracle, svc):
+    """The benchmark's reference arm builds its state and frames with the oracle's generators (it must not load the
+    engine library); they give the bytes of the engine package's generators that the GPU arm uses."""
+    from oracle.oracle import Params, State
+    for rows, rb, seed in ((2048, 4096, 1), (4096, 8192, 5)):
+        p = svc.params(rows, rb)
+        st = svc.SyntheticState.make(p, seed=seed, keep_values=True)
+        po = Params(rows, rb)
+        assert (po.part_len, po.row1_off, po.count, po.instances) == (p.part_len, p.row1_off, p.count, p.instances)
+        so = State(po, seed=seed, oracle=oracle)
+        assert np.array_equal(so.db_col, st.db_col)
+        assert np.array_equal(so.U, st.U)
+        assert all(np.array_equal(a, b) for a, b in zip(so.that, st.that))
+        assert all(np.array_equal(a, b) for a, b in zip(so.prefixes, st.prefixes))
+        assert np.array_equal(so.inv_table, st.inv_table)
+        assert np.array_equal(oracle.synthetic_requests(po, 3, seed=1000, first_client=2),
+                              svc.synthetic_requests(p, 3, seed=1000, first_client=2))

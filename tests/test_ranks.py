@@ -52,3 +52,26 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch):
     monkeypatch.setenv("RANK", "1")
     args = type("A", (), {"gpus": 2, "steps": 1, "warmup": 1, "rows": 2048, "record_bytes": 4096, "batch": 1})()
     assert bench.main_reference(args) == 0  # returns before touching any state or device
+
+
+def test_reference_arm_never_loads_the_engine_library():
+    """The reference arm builds its state and frames with the oracle's generators: the process maps only oracle/
+    libraries, and its JSON line carries the same config as the GPU arm for the same arguments."""
+    import json
+    import subprocess
+    code = (
+        "import sys, json; sys.path.insert(0, %r); import bench\n"
+        "a = bench.parse(['--impl', 'reference', '--rows', '2048', '--record-bytes', '4096', '--batch', '4',\n"
+        "                 '--steps', '2', '--warmup', '3'])\n"
+        "bench.MIN_TIMED_S = 0.05\n"
+        "bench.main_reference(a)\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print(json.dumps({'maps_engine': 'libaltopir_gpu' in maps, 'maps_ref': 'libalto_ref' in maps or\n"
+        "                  'liboracle' in maps, 'config': bench.config_dict(a)}))\n" % ROOT)
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300, cwd=ROOT)
+    assert out.returncode == 0, out.stderr
+    lines = [json.loads(x) for x in out.stdout.splitlines() if x.startswith("{")]
+    line, check = lines[0], lines[-1]
+    assert line["impl"] == "reference" and line["value"] > 0 and line["steps"] == 2 and line["warmup"] == 3
+    assert line["config"] == check["config"]
+    assert not check["maps_engine"] and check["maps_ref"]
