@@ -57,6 +57,8 @@ def _declare(L):
         "alto_ipc_import": (P, [P]),
         "alto_ipc_release": (I, [P]),
         "alto_server_new": (P, [P, S, S, I]),
+        "alto_server_new_keyed": (P, [P, S, S, I, S]),
+        "alto_server_log": (I, [P, c.POINTER(c.c_double), S]),
         "alto_server_new_loopback": (P, [S, S, S, S, I, c.c_double]),
         "alto_server_submit": (c.c_longlong, [P, P, S]),
         "alto_server_wait": (I, [P, c.c_longlong, P, S, I, c.POINTER(c.c_double)]),
@@ -94,6 +96,7 @@ EXPORTS = (
     "alto_kernel_times", "alto_engine_set_graphs", "alto_engine_set_lanes", "alto_engine_fence",
     "alto_engine_set_tuning", "alto_answer_device_noalloc",
     "alto_answer_device_parts", "alto_ipc_export", "alto_ipc_import", "alto_ipc_release", "alto_server_new",
+    "alto_server_new_keyed", "alto_server_log",
     "alto_server_new_loopback",
     "alto_server_submit", "alto_server_wait", "alto_server_stats", "alto_server_free", "alto_engine_new_empty",
     "alto_engine_load_records", "alto_engine_load_file", "alto_synthetic_db_col", "alto_synthetic_db_col_device",

@@ -1321,15 +1321,29 @@ void *create_engine(const uint8_t *db_col, size_t ld, size_t rows, size_t cols, 
     destroy(e);
     return nullptr;
   }
+  // The tail's inverse NTT runs without the reference's halving of every sum (kernels.cuh, tail_kernel): both
+  // inputs of the key-switch accumulate -- the packing matrix (through beta) and bold_t_hat -- are stored times
+  // 2^-log2(n), and the twiddles doubled, so the transform's output equals the reference's mod Q.
+  int logn = 0;
+  while ((size_t(1) << logn) < n) ++logn;
+  const uint32_t ninv = alto::inv_pow2_q(logn);
+  {
+    const size_t ntiles = e->ub_mts * e->ub_kbs;
+    alto::scale_planes_kernel<<<(unsigned)((ntiles * 1024 + 255) / 256), 256>>>(e->d_ub, ntiles, ninv);
+    if ((err = cudaGetLastError()) != cudaSuccess || (err = cudaStreamSynchronize(0)) != cudaSuccess)
+      return fail("packing matrix scaling", err);
+  }
   {
     std::vector<uint32_t> th(e->outputs * e->count);
     for (size_t o = 0; o < e->outputs; ++o)
-      for (size_t k = 0; k < e->count; ++k) th[o * e->count + k] = (uint32_t)(that[o][k] % alto::kQ);
+      for (size_t k = 0; k < e->count; ++k)
+        th[o * e->count + k] = alto::mul_q((uint32_t)(that[o][k] % alto::kQ), ninv);
     if ((err = cudaMalloc(&e->d_that, th.size() * 4)) != cudaSuccess) return fail("bold_t_hat", err);
     if ((err = cudaMemcpy(e->d_that, th.data(), th.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess)
       return fail("bold_t_hat upload", err);
     std::vector<uint32_t> tw(n);
-    for (size_t i = 0; i < n; ++i) tw[i] = (uint32_t)(inv_table[i] & 0xffffffffu);
+    // the reference multiplies by the low 32 bits of each entry (src/amx_kernels.cpp:459); doubled mod Q here
+    for (size_t i = 0; i < n; ++i) tw[i] = alto::red_q64(2 * (inv_table[i] & 0xffffffffull));
     if ((err = cudaMalloc(&e->d_tw, n * 4)) != cudaSuccess) return fail("inverse table", err);
     if ((err = cudaMemcpy(e->d_tw, tw.data(), n * 4, cudaMemcpyHostToDevice)) != cudaSuccess)
       return fail("inverse table upload", err);

@@ -174,6 +174,10 @@ __device__ __forceinline__ uint8_t *tail_dst(const TailArgs &a, int k, int slot,
 //   acc[i] = beta[i] + sum_k z[k n + i] * that[k n + i] (mod Q)                    (src/amx_kernels.cpp:500-511)
 //   inverse NTT: stages t = 1, 2, ..., n/2; block b of the stage with h = n/(2t) blocks uses table[h + b];
 //   x' = (x + y) / 2, y' = (x - y) w (mod Q)                                       (src/amx_kernels.cpp:461-498)
+// computed without the halving: a value held after s stages is 2^s times the reference's, so a stage is
+// x' = x + y, y' = (x - y) (2 w); the L = log2 n factors of 2 are cancelled in advance, since the transform is linear:
+// the engine stores beta's packing matrix and bold_t_hat multiplied by 2^-L and the twiddles doubled (engine set-up),
+// so acc enters the transform already scaled by 2^-L and leaves it equal to the reference's, mod Q.
 //   v = inter + acc, inter = (scan sum * Q + 2^31) >> 32; rescale to q1; OR the q1_bits-bit values LSB-first into
 //   the prefix from bit row1_off                                                   (src/amx_kernels.cpp:306, 515-537)
 // The stages run in rounds of three (bits s0..s0+2 of the coefficient index): in a round a thread holds the 8
@@ -197,7 +201,7 @@ __device__ __forceinline__ void tail_round(uint32_t *x, int o, int s0, int r, co
       const int i = tail_index<L>(o, m, s0, r);
       const uint32_t w = __ldg(tw + (n >> (s + 1)) + (i >> (s + 1)));
       const uint32_t a = x[m], b = x[m + t];
-      x[m] = half_q(add_q(a, b));
+      x[m] = add_q(a, b);
       x[m + t] = mul_q(sub_q(a, b), w);
     }
   }
@@ -347,7 +351,7 @@ __global__ void __launch_bounds__(128) tail_small_kernel(TailArgs a) {
       const int blk = b >> lt, j = b & (t - 1);
       const int i0 = 2 * t * blk + j, i1 = i0 + t;
       const uint32_t x = acc[i0], y = acc[i1];
-      acc[i0] = half_q(add_q(x, y));
+      acc[i0] = add_q(x, y);
       acc[i1] = mul_q(sub_q(x, y), a.twiddle[h + blk]);
     }
     __syncthreads();
@@ -368,6 +372,31 @@ __global__ void __launch_bounds__(128) tail_small_kernel(TailArgs a) {
     uint8_t *dst = tail_dst(a, k, slot, o);
     for (int b = tid; b < a.part_len; b += nt) dst[b] = (uint8_t)(res[b >> 2] >> (8 * (b & 3)));
   }
+}
+
+// Multiplies every packing-matrix value by `factor` mod Q in place, in the tile layout (tile t at t * 16 KB holds
+// rows (col, plane j) = 4 col + j of 32 columns and 128 key words): value k of column c is byte k of rows 4c..4c+3.
+// One thread per (tile, column, 4 consecutive key words): four 32-bit loads, a 4 x 4 byte transpose, four products,
+// the transpose back and four stores.
+__global__ void scale_planes_kernel(uint8_t *tiles, size_t ntiles, uint32_t factor) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t tile = idx >> 10;
+  if (tile >= ntiles) return;
+  const int c = (int)((idx >> 5) & 31), kq = (int)(idx & 31);
+  uint32_t *row = reinterpret_cast<uint32_t *>(tiles + tile * 16384 + (size_t)(4 * c) * 128) + kq;
+  const uint32_t b0 = row[0], b1 = row[32], b2 = row[64], b3 = row[96];  // planes 0..3, key words 4kq..4kq+3
+  const uint32_t lo01 = __byte_perm(b0, b1, 0x5140), hi01 = __byte_perm(b0, b1, 0x7362);
+  const uint32_t lo23 = __byte_perm(b2, b3, 0x5140), hi23 = __byte_perm(b2, b3, 0x7362);
+  uint32_t v[4] = {__byte_perm(lo01, lo23, 0x5410), __byte_perm(lo01, lo23, 0x7632), __byte_perm(hi01, hi23, 0x5410),
+                   __byte_perm(hi01, hi23, 0x7632)};
+#pragma unroll
+  for (int t = 0; t < 4; ++t) v[t] = mul_q(v[t], factor);
+  const uint32_t p01 = __byte_perm(v[0], v[1], 0x5140), p23 = __byte_perm(v[2], v[3], 0x5140);
+  const uint32_t q01 = __byte_perm(v[0], v[1], 0x7362), q23 = __byte_perm(v[2], v[3], 0x7362);
+  row[0] = __byte_perm(p01, p23, 0x5410);
+  row[32] = __byte_perm(p01, p23, 0x7632);
+  row[64] = __byte_perm(q01, q23, 0x5410);
+  row[96] = __byte_perm(q01, q23, 0x7632);
 }
 
 // ------------------------------------------------------------------------------------ synthetic database

@@ -29,9 +29,6 @@ ALTO_HD uint32_t sub_q(uint32_t a, uint32_t b) {
   return a < b ? d + kQ32 : d;
 }
 
-// s / 2 mod Q (Q odd): s / 2 when s is even, (s + Q) / 2 = (s >> 1) + (Q + 1) / 2 when s is odd.
-ALTO_HD uint32_t half_q(uint32_t s) { return (s >> 1) + ((s & 1u) ? (kQ32 + 1u) / 2u : 0u); }
-
 // x mod Q for any 64-bit x: x = h 2^32 + l = 12287 h + l (mod Q); two folds leave x < 2^32 + 2^28.
 ALTO_HD uint32_t red_q64(uint64_t x) {
   x = (x >> 32) * kFold + (x & 0xffffffffull);
@@ -44,6 +41,13 @@ ALTO_HD uint64_t fold_q64(uint64_t x) { return (x >> 32) * kFold + (x & 0xffffff
 
 // (a * b) mod Q for any 32-bit a, b.
 ALTO_HD uint32_t mul_q(uint32_t a, uint32_t b) { return red_q64((uint64_t)a * b); }
+
+// 2^-l mod Q: (Q + 1) / 2 is the inverse of 2.
+ALTO_HD uint32_t inv_pow2_q(int l) {
+  uint32_t r = 1;
+  for (int i = 0; i < l; ++i) r = mul_q(r, (kQ32 + 1u) / 2u);
+  return r;
+}
 
 // floor(u / Q) for u < 2^53.  u / 2^32 <= u / Q, so q0 = u >> 32 undershoots; the remainder u - q0 Q =
 // (u mod 2^32) + 12287 q0 < 2^32 + 2^35 leaves at most a few more multiples of Q, found the same way.

@@ -16,10 +16,14 @@ FAILED = -4     # device failure
 class Server:
     """A serving loop on an engine (engine.Engine), or on the host loopback executor when engine is None."""
 
-    def __init__(self, engine=None, max_batch=128, queue_cap=512, slots=3, request_len=None, response_len=None,
-                 service_us=0.0):
+    DEFAULT_KEYS = (1 << 64) - 1  # alto_server_new_keyed: SIZE_MAX picks the default resident table
+
+    def __init__(self, engine=None, max_batch=128, queue_cap=512, slots=2, request_len=None, response_len=None,
+                 service_us=0.0, key_bytes=DEFAULT_KEYS):
+        """key_bytes: HBM for the resident per-client table (0 = none; the default is a quarter of the free device
+        memory, at most 8 GiB)."""
         if engine is not None:
-            self.ptr = lib().alto_server_new(engine.ptr, max_batch, queue_cap, slots)
+            self.ptr = lib().alto_server_new_keyed(engine.ptr, max_batch, queue_cap, slots, key_bytes)
             self.response_len = engine.response_len()
             self.request_len = engine.request_len()
         else:
@@ -46,12 +50,22 @@ class Server:
             return st, (out if st == 0 else None), lat.value
         return st, (out if st == 0 else None)
 
+    STATS = ("answered", "rejected", "busy", "failed", "batches", "mean_batch", "p50_ms", "p99_ms", "p999_ms",
+             "max_ms", "queued", "resident_hits", "admitted", "evicted", "uncached", "table_rows")
+    LOG = ("t_dispatch", "t_done", "taken", "on_device", "packed", "resident", "upload_ms", "pack_ms", "rest_ms",
+           "device_ms")
+
     def stats(self):
-        v = (ctypes.c_double * 11)()
-        lib().alto_server_stats(self.ptr, v, 11)
-        keys = ("answered", "rejected", "busy", "failed", "batches", "mean_batch", "p50_ms", "p99_ms", "p999_ms",
-                "max_ms", "queued")
-        return dict(zip(keys, list(v)))
+        v = (ctypes.c_double * len(self.STATS))()
+        lib().alto_server_stats(self.ptr, v, len(self.STATS))
+        return dict(zip(self.STATS, list(v)))
+
+    def log(self, max_rows=65536):
+        """The per-batch log, oldest first: a list of dicts with the LOG fields."""
+        buf = (ctypes.c_double * (max_rows * len(self.LOG)))()
+        n = lib().alto_server_log(self.ptr, buf, max_rows)
+        w = len(self.LOG)
+        return [dict(zip(self.LOG, buf[k * w:(k + 1) * w])) for k in range(max(n, 0))]
 
     def close(self):
         if getattr(self, "ptr", None):

@@ -63,6 +63,8 @@ def parse(argv=None):
     ap.add_argument("--serve-seconds", type=float, default=3.0)
     ap.add_argument("--serve-clients", type=int, default=4096, help="seeded clients whose frames are replayed")
     ap.add_argument("--max-batch", type=int, default=1024)
+    ap.add_argument("--serve-slots", type=int, default=2, help="device batch contexts of the serving loop")
+    ap.add_argument("--serve-queue", type=int, default=2048, help="frames the serving loop's pinned pool holds")
     ap.add_argument("--lanes", type=int, default=2,
                     help="batch contexts the device-resident loop rotates through (1..4; consecutive batches overlap)")
     ap.add_argument("--shard", action="store_true",
@@ -668,8 +670,9 @@ def main_ours(a):
 # ------------------------------------------------------------------------------------------------ serving mode
 def main_serve(a):
     """Open-loop serving: Poisson arrivals at each offered rate into the continuous-batching loop (max_batch
-    a.max_batch, three device batch contexts) and into a one-query-per-batch loop, answered QPS and latency
-    percentiles from submit to completion.  One JSON line."""
+    a.max_batch, --serve-slots device batch contexts, the resident client table at its default size) and into a
+    one-query-per-batch loop, answered QPS and latency percentiles from submit to completion, plus the loop's own
+    statistics and a summary of its per-batch log.  One JSON line."""
     import torch
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     import __graft_entry__ as ge
@@ -677,17 +680,30 @@ def main_serve(a):
     from altopir_b200 import engine as eng, service as svc, server as srv
     eng.init()
     p = svc.params(a.rows, a.record_bytes)
-    st = svc.SyntheticState.make(p, seed=1, keep_values=False)
-    e = eng.Engine.from_state(st, threads=svc.threads(), tile=a.rows * a.record_bytes <= (8 << 30))
+    st = svc.SyntheticState.make(p, seed=1, keep_values=False, host_db=False)
+    e = eng.Engine.from_state(st, threads=svc.threads(), tile=False)
     st.ub = None
-    frames = svc.synthetic_requests(p, a.serve_clients, seed=2024)
+    # the clients' frames, generated on the device in pieces and kept in host memory
+    ql = e.request_len()
+    stride = (7 + ql + 255) // 256 * 256
+    frames = np.empty((a.serve_clients, ql), dtype=np.uint8)
+    piece = max(1, min(a.serve_clients, (4 << 30) // stride))
+    slots = torch.zeros((piece, stride), dtype=torch.uint8, device="cuda")
+    for c0 in range(0, a.serve_clients, piece):
+        n = min(piece, a.serve_clients - c0)
+        torch.cuda.synchronize()
+        svc.synthetic_requests_device(p, n, 2024, slots.data_ptr(), stride, first_client=c0)
+        frames[c0:c0 + n] = slots[:n, 7:7 + ql].cpu().numpy()
+    del slots
+    torch.cuda.empty_cache()
     rates = [float(x) for x in a.serve.split(",")]
     print(f"serve: engine and {a.serve_clients} frames ready", file=sys.stderr, flush=True)
     rows = []
     for label, mb in (("batched", a.max_batch), ("plain", 1)):
-        s = srv.Server(e, max_batch=mb, queue_cap=max(4 * a.max_batch, 4096), slots=3)
+        s = srv.Server(e, max_batch=mb, queue_cap=a.serve_queue, slots=a.serve_slots)
         for rate in rates:
-            s.stats()
+            before = s.stats()
+            nlog = len(s.log())
             t0 = time.time()
             res, offered, elapsed = srv.poisson_load(s, frames, rate, a.serve_seconds, seed=int(rate), clients=8)
             print(f"serve {label} {rate:g} QPS offered: {offered} requests in {time.time() - t0:.1f} s",
@@ -695,17 +711,25 @@ def main_serve(a):
             lat = sorted(r[3] * 1e3 for r in res if r[1] == 0)
             ok = len(lat)
             pct = lambda q: lat[min(len(lat) - 1, int(q * len(lat)))] if lat else None
+            after = s.stats()
+            log = s.log()[nlog:]
+            dev = sorted(r["device_ms"] for r in log)
             rows.append({"loop": label, "offered_qps": rate, "requests": offered, "answered": ok,
                          "busy": sum(1 for r in res if r[1] == srv.BUSY),
                          "answered_qps": ok / elapsed, "elapsed_s": elapsed, "p50_ms": pct(0.5), "p99_ms": pct(0.99),
-                         "p999_ms": pct(0.999)})
+                         "p999_ms": pct(0.999),
+                         "batches": len(log), "mean_batch": (sum(r["on_device"] for r in log) / len(log)) if log else 0,
+                         "batch_device_ms_p50": dev[len(dev) // 2] if dev else None,
+                         "resident_frames": after["resident_hits"] - before["resident_hits"],
+                         "packed_frames": sum(r["packed"] for r in log)})
         rows[-1]["loop_stats"] = s.stats()
         s.close()
     line = {"metric": "serving: answered QPS and p50/p99/p99.9 latency (submit to response) under open-loop "
                       "Poisson arrivals", "unit": "QPS", "n_gpus": 1, "data": "synthetic",
             "config": {"workload": f"continuous batching over a {a.rows * a.record_bytes / 2**30:g} GiB database, "
                                    f"{a.serve_clients} seeded clients, {a.serve_seconds} s per rate",
-                       "rows": a.rows, "record_bytes": a.record_bytes, "max_batch": a.max_batch, "slots": 3},
+                       "rows": a.rows, "record_bytes": a.record_bytes, "max_batch": a.max_batch,
+                       "slots": a.serve_slots, "queue": a.serve_queue},
             "rates": rows}
     print(json.dumps(line))
     e.close()
@@ -713,13 +737,72 @@ def main_serve(a):
 
 
 # ------------------------------------------------------------------------------------------------ column shards
+class CudaTimer:
+    """Device time of a stretch of work on torch's current stream (CUDA events)."""
+
+    def __init__(self, torch):
+        self.torch = torch
+        self.s, self.e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def sync(self):
+        self.torch.cuda.synchronize()
+
+    def start(self):
+        self.s.record()
+
+    def stop(self):
+        self.e.record()
+        self.torch.cuda.synchronize()
+        return self.s.elapsed_time(self.e)
+
+
+class HostTimer:
+    """Wall time of a stretch of host work (the CPU ranks of the tests)."""
+
+    def sync(self):
+        pass
+
+    def start(self):
+        self.t0 = time.perf_counter()
+
+    def stop(self):
+        return 1e3 * (time.perf_counter() - self.t0)
+
+
+def shard_timed(step, timer, steps, warmup, world, device):
+    """--shard timing: warm-up steps, a barrier, then exactly `steps` steps timed on this rank; max over ranks."""
+    import torch.distributed as dist
+    for _ in range(max(3, warmup)):
+        step()
+    timer.sync()
+    dist.barrier()
+    timer.start()
+    for _ in range(steps):
+        step()
+    return max_over_ranks(timer.stop(), world, device=device)
+
+
+def shard_line(a, world, ranges, ms, ms_nccl, exact):
+    """Rank 0's JSON line of --shard: the whole job answers --batch queries per step (every rank answers the same
+    frames for its parts), so `value` is strong scaling."""
+    cfg = config_dict(a)
+    return {"metric": METRIC, "value": a.batch * a.steps / (ms * 1e-3), "unit": "QPS", "n_gpus": world,
+            "steps": a.steps, "warmup": max(3, a.warmup), "ms_per_step": ms / a.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "u8 x u8 limbs -> int32 (exact)", "data": "synthetic",
+            "config": cfg, "parallelism": f"columns{world}", "output_ranges": ranges, "mode": "column shards",
+            "exchange": "frames broadcast from rank 0; each rank's tail kernel writes its parts into every rank's "
+                        "response buffer (CUDA IPC mappings), then one barrier",
+            "nccl_all_gather": {"value": a.batch * a.steps / (ms_nccl * 1e-3), "unit": "QPS",
+                                "ms_per_step": ms_nccl / a.steps},
+            "byte_exact": exact}
+
+
 def main_shard(a):
     """Column sharding (altopir_b200.shard): rank r holds the columns of its output range; every step rank 0's batch
     of frames is broadcast and each rank's tail kernel writes its parts into every rank's response buffer (CUDA IPC
-    mappings; shard.PeerGather), so that after one barrier every rank holds the full responses.  The whole job
-    answers --batch queries per step, so `value` is strong scaling; timed on the device, max over ranks.  Beside it,
-    `nccl_all_gather` times the same answer followed by an NCCL all_gather of the parts.  Rank 0 checks both
-    against a whole engine (byte-exact)."""
+    mappings; shard.PeerGather), so that after one barrier every rank holds the full responses.  Timed on the device,
+    max over ranks.  Beside it, `nccl_all_gather` times the same answer followed by an NCCL all_gather of the parts.
+    Rank 0 checks both against a whole engine (byte-exact)."""
     import torch
     import torch.distributed as dist
     from datetime import timedelta
@@ -749,24 +832,11 @@ def main_shard(a):
     # mappings, NVLink stores between GPUs); the baseline beside it: answer locally, then NCCL all_gather
     fused = shard.PeerGather(e, ranges, part_len, B)
     gathered = shard.ShardedAnswerer(shard.engine_local(e), ranges, part_len, "cuda")
-    s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-
-    def timed(step):
-        for _ in range(max(3, a.warmup)):
-            step()
-        torch.cuda.synchronize()
-        dist.barrier()
-        s_ev.record()
-        for _ in range(a.steps):
-            step()
-        e_ev.record()
-        torch.cuda.synchronize()
-        return max_over_ranks(s_ev.elapsed_time(e_ev), world)
-
-    ms = timed(lambda: fused.answer(slots, stride, B, src=0))
+    timer = CudaTimer(torch)
+    ms = shard_timed(lambda: fused.answer(slots, stride, B, src=0), timer, a.steps, a.warmup, world, "cuda")
     status, resp = fused.answer(slots, stride, B, src=0)
     resp = resp.clone()
-    ms_nccl = timed(lambda: gathered.answer(slots, stride, B))
+    ms_nccl = shard_timed(lambda: gathered.answer(slots, stride, B), timer, a.steps, a.warmup, world, "cuda")
     _, resp_nccl = gathered.answer(slots, stride, B)
     fused.close()
     exact = None
@@ -781,18 +851,7 @@ def main_shard(a):
         full.close()
     dist.barrier()
     if rank == 0:
-        value = B * a.steps / (ms * 1e-3)  # the job's queries: every rank answers the same batch for its parts
-        cfg = config_dict(a)
-        cfg.update({"parallelism": f"columns{world}", "output_ranges": ranges,
-                    "exchange": "frames broadcast from rank 0; each rank's tail kernel writes its parts into every "
-                                "rank's response buffer (CUDA IPC mappings), then one barrier"})
-        print(json.dumps({"metric": METRIC, "value": value, "unit": "QPS", "n_gpus": world, "steps": a.steps,
-                          "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
-                          "scaling": "strong", "vs_baseline": None, "dtype": "u8 x u8 limbs -> int32 (exact)",
-                          "data": "synthetic", "config": cfg, "mode": "column shards",
-                          "nccl_all_gather": {"value": B * a.steps / (ms_nccl * 1e-3), "unit": "QPS",
-                                              "ms_per_step": ms_nccl / a.steps},
-                          "byte_exact": exact}))
+        print(json.dumps(shard_line(a, world, ranges, ms, ms_nccl, exact)))
     e.close()
     dist.destroy_process_group()
     return 0

@@ -183,35 +183,53 @@ int alto_kernel_times(void *engine, double *ms, long long *batches, int reset);
 int alto_answer_device_noalloc(void *engine, const uint8_t *d_req, size_t req_stride, size_t b, uint8_t *d_out,
                                size_t out_stride, int *d_status);
 
-/* Serving loop with continuous batching over one engine (the engine loop of src/bin/altopir.rs:245-513 without the
- * TCP front end).  Frames submitted from any thread wait in a FIFO of queue_cap entries; a batcher thread takes
- * whatever is queued, up to max_batch, as soon as one of `slots` device batch contexts (1..8) is free -- it never
- * holds a request back to fill a batch -- and answers it on that context's stream, so up to `slots` batches upload
- * and compute concurrently.  Each context keeps its frames, limbs, sums and responses resident in device memory,
- * sized for max_batch frames at creation: admission to the device is by free context.
- *   alto_server_new        returns NULL for bad arguments (1 <= slots <= 8) or when the device memory is short.
- *   alto_server_submit     copies the frame and returns a ticket >= 0, -9 when the queue is full (the reference
- *                          server's BUSY status 9), -1 for bad arguments.
+/* Serving loop with continuous batching over one engine (the engine loop of src/bin/altopir.rs:403-510 without the
+ * TCP front end).  alto_server_submit copies a frame into a pinned pool of queue_cap frames (outside the loop's lock);
+ * a batcher thread takes whatever is queued, up to max_batch, as soon as one of `slots` device batch contexts (1..8)
+ * is free -- it never holds a request back to fill a batch, and frames that arrive while every context is busy join
+ * the next batch -- and answers it on that context's stream, so up to `slots` batches upload and compute at once.
+ * Per-client state in HBM: the pack product beta = y U of a client's packing keys y depends on nothing else, so the
+ * loop keeps it in a resident table of key_bytes / (cols * 4) rows.  A frame whose y keys equal, byte for byte, those
+ * of a resident client skips the pack GEMM and gathers its row; a new client is admitted to a free row, or to the
+ * least recently used row that no batch in flight uses, and its batch stores its beta there (valid frames only).
+ * When no row can be had the frame is answered all the same, with its pack computed and not kept.  Responses are
+ * the same bytes either way.
+ *   alto_server_new_keyed  returns NULL for bad arguments (1 <= slots <= 8, queue_cap <= 2^30) or when the device
+ *                          or pinned host memory is short; key_bytes = 0 disables the table, SIZE_MAX picks the
+ *                          default (a quarter of the free device memory, at most 8 GiB).
+ *   alto_server_new        alto_server_new_keyed with the default table.
+ *   alto_server_submit     copies the frame and returns a ticket >= 0, -9 when the pool is full (the reference
+ *                          server's BUSY status 9), -1 for bad arguments.  A frame of the wrong length gets a ticket
+ *                          that completes at once with status 1.
  *   alto_server_wait       waits up to timeout_ms for a ticket; returns its status (0..3 as alto_answer, with the
  *                          response copied to out for 0), -4 on a device failure, -5 on timeout (the ticket stays
  *                          valid), -1 for an unknown ticket; *latency_ms (if not NULL) receives the time from
  *                          submit to completion measured by the loop.  A completed ticket is released by this call.
- *   alto_server_stats      out[0..10] = answered, rejected (status 1..3), busy, failed, batches, mean batch size,
- *                          latency p50, p99, p99.9 and max in ms (submit to completion), frames still queued.
- *   alto_server_free       answers everything queued, then stops the threads and frees the contexts.
+ *   alto_server_stats      out[0..15] = answered, rejected (status 1..3), busy, failed, batches, mean batch size,
+ *                          latency p50, p99, p99.9 and max in ms (submit to completion), frames still queued,
+ *                          frames answered from resident rows, clients admitted, rows evicted, frames answered
+ *                          without a row (table full of rows in use), table rows.
+ *   alto_server_log        the per-batch log (src/bin/altopir.rs:472-510, --log): up to max_rows of the most recent
+ *                          batches, oldest first, 10 doubles each: dispatch and completion time (s, the loop's
+ *                          clock), frames taken, frames on the device, frames that ran the pack, frames answered from
+ *                          resident rows, device ms of the upload, of the pack and row gather, of the scan, tails
+ *                          and download, and in total.  Returns the number of rows written, -1 for bad arguments.
+ *   alto_server_free       answers everything queued, then stops the threads and frees the contexts and the table.
  * alto_server_new_loopback builds the same loop without an engine: batches are answered on the host after
  * service_us microseconds by a deterministic function of the frame, to test queueing and batching without a
- * device.  Both have no counterpart in the reference's C ABI.
+ * device.  None of these has a counterpart in the reference's C ABI.
  * The loop answers in batch contexts of its own, so while it runs, one other thread may still call alto_answer,
  * alto_answer_device or alto_enqueue_device on the same engine; alto_engine_set_tuning, alto_engine_set_graphs,
  * the ingest calls and alto_engine_free must wait until alto_server_free has returned. */
 void *alto_server_new(void *engine, size_t max_batch, size_t queue_cap, int slots);
+void *alto_server_new_keyed(void *engine, size_t max_batch, size_t queue_cap, int slots, size_t key_bytes);
 void *alto_server_new_loopback(size_t request_len, size_t response_len, size_t max_batch, size_t queue_cap, int slots,
                                double service_us);
 long long alto_server_submit(void *server, const uint8_t *frame, size_t len);
 int alto_server_wait(void *server, long long ticket, uint8_t *out, size_t out_len, int timeout_ms,
                      double *latency_ms);
 int alto_server_stats(void *server, double *out, size_t n);
+int alto_server_log(void *server, double *out, size_t max_rows);
 void alto_server_free(void *server);
 
 /* A database too large to hold in host memory in column order, or stored on disk record by record, is loaded

@@ -66,3 +66,60 @@ def test_direct_answers_beside_a_running_loop(gpu, svc, eng):
     assert s.stats()["failed"] == 0
     s.close()
     e.close()
+
+
+@pytest.mark.timeout(300, method="thread")
+def test_resident_clients_skip_the_pack_and_answer_the_same(gpu, svc, eng):
+    """Clients whose packing keys y are resident skip the pack GEMM: with a table of four rows, ten clients sending
+    new queries with their own keys again and again are answered exactly as the engine answers each frame alone,
+    rows are admitted, reused and evicted, a frame with a y key >= Q (status 3) is never kept, and the per-batch log
+    accounts for every frame."""
+    from altopir_b200 import server as srv
+    p = svc.params(2048, 4096)
+    st = svc.SyntheticState.make(p, seed=91, full_prefix=True)
+    e = eng.Engine.from_state(st)
+    base = svc.synthetic_requests(p, 10, seed=92)
+    queries = svc.synthetic_requests(p, 60, seed=93)
+    q0 = 9 + 8 * p.count
+    frames = []
+    for k in range(60):  # client k % 10 with the query words of frame k
+        f = base[k % 10].copy()
+        f[q0:] = queries[k][q0:]
+        frames.append(f)
+    bad = base[3].copy()
+    bad[9:13] = 0xFF  # first y key word >= Q
+    frames.append(bad)
+    rl = e.response_len()
+    alone = []
+    for f in frames:
+        out = np.zeros((1, rl), dtype=np.uint8)
+        status = np.full(1, -1, dtype=np.int32)
+        e.answer([f], out, status)
+        alone.append((int(status[0]), out[0].copy()))
+    assert alone[-1][0] == 3
+    row_bytes = p.record_bytes * 4
+    for key_bytes, expect_hits in ((4 * row_bytes, True), (0, False)):
+        s = srv.Server(e, max_batch=8, queue_cap=128, slots=2, key_bytes=key_bytes)
+        for rnd in range(3):
+            order = list(range(len(frames)))
+            np.random.default_rng(rnd).shuffle(order)
+            tickets = [(i, s.submit(frames[i])) for i in order]
+            for i, t in tickets:
+                code, resp = s.wait(t)
+                assert code == alone[i][0], (key_bytes, rnd, i)
+                if code == 0:
+                    assert np.array_equal(resp, alone[i][1]), (key_bytes, rnd, i)
+        stats = s.stats()
+        log = s.log()
+        assert stats["failed"] == 0 and stats["answered"] == 3 * 60 and stats["rejected"] == 3
+        assert len(log) == stats["batches"]
+        assert all(r["packed"] + r["resident"] == r["on_device"] <= r["taken"] <= 8 for r in log)
+        assert sum(r["on_device"] for r in log) == 3 * 61
+        assert sum(r["resident"] for r in log) == stats["resident_hits"]
+        if expect_hits:
+            assert stats["table_rows"] == 4 and stats["resident_hits"] > 0 and stats["evicted"] > 0
+            assert stats["admitted"] >= 10
+        else:
+            assert stats["table_rows"] == 0 and stats["resident_hits"] == 0 and stats["admitted"] == 0
+        s.close()
+    e.close()

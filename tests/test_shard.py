@@ -84,9 +84,18 @@ def _rank(rank, world, port, out):
 
     ans = shard.ShardedAnswerer(local, ranges, st.prefixes[0].size, "cpu")
     status, resp = ans.answer(slots, stride, b)
+    # bench.py --shard's rank logic on these ranks: timed steps (max over ranks) and rank 0's JSON line
+    import bench
+    a = bench.parse(["--shard", "--rows", "2048", "--record-bytes", "8192", "--batch", str(b), "--steps", "2",
+                     "--warmup", "1"])
+    ms = bench.shard_timed(lambda: ans.answer(slots, stride, b), bench.HostTimer(), a.steps, a.warmup, world, "cpu")
     if rank == 0:
         r, st0, full = orc.answer(st, [slots[c, 7:7 + ql].numpy() for c in range(b)])
+        line = bench.shard_line(a, world, ranges, ms, ms, {"nccl_vs_whole_engine": True})
         out[0] = bool(np.array_equal(resp.numpy(), full)) and list(status) == list(st0)
+        out[1] = (line["n_gpus"] == world and line["scaling"] == "strong" and line["steps"] == 2 and
+                  line["warmup"] == 3 and abs(line["value"] - b * 2 / (ms * 1e-3)) < 1e-6 * line["value"] and
+                  line["output_ranges"] == ranges and line["config"] == bench.config_dict(a))
     dist.destroy_process_group()
 
 
@@ -102,4 +111,4 @@ def test_gloo_ranks_gather_full_responses(world):
         for p in procs:
             p.join(180)
             assert p.exitcode == 0
-        assert out[0] is True
+        assert out[0] is True and out[1] is True
