@@ -3,7 +3,7 @@ or CTA-pair kernels, wide scan units, limb-column tile cap, scan split target) o
 that it returns the same bytes as the built-in plan, and write the fastest into tuning.txt next to the library,
 which alto_engine_new loads.
 
-    python altopir-public_b200/autotune.py --rows 32768,262144 [--out altopir-public_b200/tuning.txt]
+    python altopir-public_b200/autotune.py --rows 32768,262144 [--out altopir-public_b200/tuning.txt] [--merge]
 """
 import argparse
 import datetime
@@ -56,6 +56,7 @@ def main():
     ap.add_argument("--rounds", type=int, default=3)
     ap.add_argument("--margin", type=float, default=0.03, help="required gain over the built-in plan")
     ap.add_argument("--out", default=os.path.join(HERE, "tuning.txt"))
+    ap.add_argument("--merge", action="store_true", help="keep the rows of other database sizes already in --out")
     a = ap.parse_args()
     import torch
     import __graft_entry__ as ge
@@ -66,16 +67,16 @@ def main():
     lines = []
     for rows in [int(x) for x in a.rows.split(",")]:
         p = svc.params(rows, a.record_bytes)
-        st = svc.SyntheticState.make(p, seed=5, keep_values=False)
-        e = eng.Engine.from_state(st, threads=svc.threads(), tile=rows * a.record_bytes <= (8 << 30))
+        st = svc.SyntheticState.make(p, seed=5, keep_values=False, host_db=False)  # database made on the device
+        e = eng.Engine.from_state(st, threads=svc.threads(), tile=False)
         e.set_tuning([])
         nchunks = (rows + 32767) // 32768
         bmax = max(buckets)
-        frames = svc.synthetic_requests(p, bmax, seed=6)
         ql, rl = e.request_len(), e.response_len()
         stride = (7 + ql + 255) // 256 * 256
         slots = torch.zeros((bmax, stride), dtype=torch.uint8, device="cuda")
-        slots[:, 7:7 + ql] = torch.from_numpy(frames).cuda()
+        torch.cuda.synchronize()
+        svc.synthetic_requests_device(p, bmax, 6, slots.data_ptr(), stride)
         d_out = torch.zeros((bmax, rl), dtype=torch.uint8, device="cuda")
         for b in buckets:
             e.set_tuning([])
@@ -107,10 +108,23 @@ def main():
         del slots, d_out
         torch.cuda.empty_cache()
     gpu = torch.cuda.get_device_name(0)
+    tuned = {int(x) for x in a.rows.split(",")}
+    head = [f"# GEMM plans chosen by autotune.py on {gpu}, {datetime.date.today()}, record bytes {a.record_bytes}",
+            f"# command: python altopir-public_b200/autotune.py --rows {a.rows} ({a.rounds} interleaved rounds, "
+            f"medians, {a.margin:.0%} margin)"]
+    kept = []
+    if a.merge and os.path.exists(a.out):  # rows of other database sizes stay as they were
+        with open(a.out) as f:
+            for line in f:
+                if line.startswith("#"):
+                    if "rows_max" not in line:
+                        head.append(line.rstrip("\n"))
+                    continue
+                if line.split() and int(line.split()[0]) not in tuned:
+                    kept.append(line.rstrip("\n"))
     with open(a.out, "w") as f:
-        f.write(f"# GEMM plans chosen by autotune.py on {gpu}, {datetime.date.today()}, record bytes "
-                f"{a.record_bytes}\n# rows_max b_max pair wide bn_cap units_per_pair\n")
-        f.write("\n".join(lines) + "\n")
+        f.write("\n".join(head) + "\n# rows_max b_max pair wide bn_cap units_per_pair\n")
+        f.write("\n".join(sorted(kept + lines, key=lambda x: (int(x.split()[0]), int(x.split()[1])))) + "\n")
     print("wrote", a.out)
 
 

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/altopir_gpu.h"
+#include "hint.cuh"
 #include "kernels.cuh"
 #include "limb_gemm2.cuh"
 
@@ -273,6 +274,9 @@ struct Engine {
   // (5, 4, 5 and 2 of 16 parts) measured fastest with 6,4,3,2,1 (1.10 ms a call); 6,5,3,2, 5,5,4,2, 8,4,4, 8,4,2,2,
   // 8,4,2,1,1 and 7,5,3,1 took 1.11-1.14 ms: what they save after the last scan, their smaller groups' scans cost.
   std::vector<int> host_weights = {2, 2, 2, 1};
+  // alto_answer: the tails of this many groups before the last run on the batch's stream between their scan and the
+  // next group's, instead of beside the next scan (ALTO_HOST_INLINE)
+  int host_inline = 0;
   std::vector<TuneEntry> tuning;  // sorted by b_max; the first entry with b_max >= batch size applies
 };
 
@@ -799,10 +803,12 @@ bool enqueue_query_split(const Engine *e, const Batch *bt, const uint8_t *d_slot
 // Scan and tail in column groups: the tail of every group but the last runs on the side stream beside the scan of the
 // next group (the tail is integer-ALU work, the scan tensor work; the side stream's lower priority lets the scan's
 // CTAs be placed first); `done[g]`, when given, is recorded after the tail of group g.
+// Groups g >= inline_from run their tail on the batch's stream right after their scan (before the next group's
+// scan), so that their responses are complete, and can download, while the next group computes.
 bool enqueue_scan_tails(Engine *e, Batch *bt, const Plan &p, const CUtensorMap &map_q, const uint8_t *d_slots,
                         size_t slot_stride, size_t slots, uint8_t *resp, size_t resp_stride, const Groups &gr,
                         const cudaEvent_t *done, int *launches, cudaEvent_t before_last_tail = nullptr,
-                        cudaEvent_t last_tail_after = nullptr) {
+                        cudaEvent_t last_tail_after = nullptr, int inline_from = 8) {
   cudaStream_t st = bt->st;
   bool forked = false;
   for (int g = 0; g < gr.count; ++g) {
@@ -812,7 +818,7 @@ bool enqueue_scan_tails(Engine *e, Batch *bt, const Plan &p, const CUtensorMap &
                                                 parts * gr.tiles_per_part);
     if (!ok) return false;
     const bool last = g + 1 == gr.count;
-    cudaStream_t ts = last ? st : bt->side;
+    cudaStream_t ts = (last || g >= inline_from) ? st : bt->side;
     if (ts != st) {
       ALTO_CK(cudaEventRecord(bt->ev_scan[g], st));
       ALTO_CK(cudaStreamWaitEvent(ts, bt->ev_scan[g], 0));
@@ -820,7 +826,7 @@ bool enqueue_scan_tails(Engine *e, Batch *bt, const Plan &p, const CUtensorMap &
     } else if (last && before_last_tail) {
       ALTO_CK(cudaEventRecord(before_last_tail, st));
     }
-    if (last && last_tail_after) ALTO_CK(cudaStreamWaitEvent(st, last_tail_after, 0));
+    if (last_tail_after && ts == st) ALTO_CK(cudaStreamWaitEvent(st, last_tail_after, 0));
     ALTO_CK(alto::launch_tail(tail_args(e, bt, d_slots, slot_stride, resp, resp_stride, o0, parts), slots, ts));
     *launches += 2;
     if (done) ALTO_CK(cudaEventRecord(done[g], ts));
@@ -1133,7 +1139,7 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
   ALTO_H(cudaEventRecord(e->ev_status, vs));
   if (e->overlap) ALTO_H(cudaStreamWaitEvent(st, bt->ev_qready, 0));
   if (!enqueue_scan_tails(e, bt, p, map_q, bt->d_req, e->slot_stride, nc, bt->d_resp, e->resp_len, groups,
-                          e->ev_group, &launches, nullptr, e->ev_status))
+                          e->ev_group, &launches, nullptr, e->ev_status, groups.count - e->host_inline - 1))
     return -4;
   // the error word comes back behind the last tail, so the final synchronisation covers it
   ALTO_H(cudaMemcpyAsync(bt->h_err, bt->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
@@ -1283,6 +1289,7 @@ void *create_engine(const uint8_t *db_col, size_t ld, size_t rows, size_t cols, 
   if (const char *v = getenv("ALTO_OVERLAP")) e->overlap = v[0] != '0';
   if (const char *v = getenv("ALTO_GROUPS")) e->groups = std::max(1, std::min(8, atoi(v)));
   if (const char *v = getenv("ALTO_HOST_GROUPS")) e->host_weights = group_weights(atoi(v), true);
+  if (const char *v = getenv("ALTO_HOST_INLINE")) e->host_inline = std::max(0, std::min(7, atoi(v)));
   if (const char *v = getenv("ALTO_HOST_WEIGHTS")) {
     std::vector<int> w = parse_weights(v);
     if (!w.empty()) e->host_weights = w;
@@ -1678,6 +1685,58 @@ int alto_synthetic_db_col_device(uint8_t *d_db, size_t ld, size_t rows, size_t c
   if (e != cudaSuccess) {
     set_error("synthetic database", e);
     return -1;
+  }
+  return 0;
+}
+
+int alto_hint_ring(void *p, const uint64_t *query, uint64_t *out, int perm_out) {
+  Engine *e = static_cast<Engine *>(p);
+  if (!e || !query || !out) {
+    set_error("alto_hint_ring: bad arguments");
+    return -1;
+  }
+  std::vector<uint32_t> psi, psi_inv;
+  uint32_t n_inv = 0;
+  if (e->rows % e->n || !alto::hint_tables((int)e->n, psi, psi_inv, n_inv)) {
+    set_error("alto_hint_ring: needs records a multiple of n and n a power of two <= 2048");
+    return -1;
+  }
+  if (cudaSetDevice(e->dev) != cudaSuccess) return -4;
+  const size_t n = e->n, polys = e->rows / n;
+  uint64_t *d_query = nullptr, *d_out = nullptr;
+  uint32_t *d_qhat = nullptr, *d_psi = nullptr, *d_psi_inv = nullptr;
+  cudaError_t err = cudaSuccess;
+  auto step = [&](cudaError_t x) {
+    if (err == cudaSuccess) err = x;
+  };
+  step(cudaMalloc(&d_query, e->rows * sizeof(uint64_t)));
+  step(cudaMalloc(&d_qhat, e->rows * sizeof(uint32_t)));
+  step(cudaMalloc(&d_psi, n * sizeof(uint32_t)));
+  step(cudaMalloc(&d_psi_inv, n * sizeof(uint32_t)));
+  step(cudaMalloc(&d_out, n * e->cols * sizeof(uint64_t)));
+  step(cudaMemcpy(d_query, query, e->rows * sizeof(uint64_t), cudaMemcpyHostToDevice));
+  step(cudaMemcpy(d_psi, psi.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  step(cudaMemcpy(d_psi_inv, psi_inv.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  const unsigned threads = (unsigned)std::max<size_t>(32, std::min<size_t>(256, n / 2));
+  if (err == cudaSuccess) {
+    alto::hint_query_kernel<<<(unsigned)polys, threads, n * sizeof(uint32_t)>>>(d_query, (int)n, d_psi, n_inv,
+                                                                               d_qhat);
+    step(cudaGetLastError());
+  }
+  if (err == cudaSuccess) {
+    alto::hint_ring_kernel<<<(unsigned)e->cols, threads, 2 * n * sizeof(uint32_t)>>>(
+        e->d_db, e->db_kbs, (int)n, (int)polys, d_qhat, d_psi, d_psi_inv, d_out, e->cols, perm_out);
+    step(cudaGetLastError());
+  }
+  step(cudaMemcpy(out, d_out, n * e->cols * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  cudaFree(d_query);
+  cudaFree(d_qhat);
+  cudaFree(d_psi);
+  cudaFree(d_psi_inv);
+  cudaFree(d_out);
+  if (err != cudaSuccess) {
+    set_error("alto_hint_ring", err);
+    return -4;
   }
   return 0;
 }

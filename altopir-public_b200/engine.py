@@ -75,6 +75,7 @@ class Engine:
         inv = np.ascontiguousarray(inv_table, dtype=np.uint64)
         db_col = np.ascontiguousarray(db_col)
         ub = np.ascontiguousarray(ub)
+        self.rows, self.cols = rows, cols
         self.ptr = lib().alto_engine_new(_p(db_col), _p(tiled.buf), ld, rows, cols, _p(ub), n, tg, _ptrs(pre),
                                          part_len, row1_off, q1, q1_bits, _ptrs(that64), _p(inv), q, threads)
         if not self.ptr:
@@ -86,6 +87,7 @@ class Engine:
         load_records or load_file (the reference server's streaming reader, src/server.rs:380-500)."""
         assert ub.size == 4 * tg * n * cols and len(prefixes) == cols // n and len(that) == cols // n
         self = cls.__new__(cls)
+        self.rows, self.cols = rows, cols
         pre = [np.ascontiguousarray(p, dtype=np.uint8) for p in prefixes]
         that64 = [np.ascontiguousarray(t, dtype=np.uint64) for t in that]
         inv = np.ascontiguousarray(inv_table, dtype=np.uint64)
@@ -108,6 +110,18 @@ class Engine:
         r = lib().alto_engine_load_file(self.ptr, os.fsencode(path), num_real_rows)
         if r < 0:
             raise EngineError(f"engine error {r}: {last_error()}")
+
+    def hint_ring(self, query, perm_out=False):
+        """alto_hint_ring: the offline hint's ring multiply over the resident database (YServer::answer_hint_ring,
+        src/server.rs:656-768).  query: (rows / n, n) raw query polynomials; returns the (n, cols) uint64 hint."""
+        q = np.ascontiguousarray(query, dtype=np.uint64)
+        n = q.shape[1]
+        assert q.shape[0] * n == self.rows, "one raw polynomial per n records"
+        out = np.empty((n, self.cols), dtype=np.uint64)
+        r = lib().alto_hint_ring(self.ptr, _p(q), _p(out), int(perm_out))
+        if r < 0:
+            raise EngineError(f"engine error {r}: {last_error()}")
+        return out
 
     def fill_synthetic(self):
         """alto_engine_fill_synthetic: the whole database becomes the synthetic records, generated on the device."""

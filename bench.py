@@ -67,6 +67,9 @@ def parse(argv=None):
     ap.add_argument("--serve-queue", type=int, default=2048, help="frames the serving loop's pinned pool holds")
     ap.add_argument("--lanes", type=int, default=2,
                     help="batch contexts the device-resident loop rotates through (1..4; consecutive batches overlap)")
+    ap.add_argument("--profile", type=int, default=0, metavar="N",
+                    help="profiling run for ncu: N batches of the headline configuration through alto_enqueue_device "
+                         "(direct launches) and N through alto_answer after the warm-up, no timing loops, no JSON")
     ap.add_argument("--shard", action="store_true",
                     help="column sharding: the ranks split the outputs of one engine state and answer every batch "
                          "together (strong scaling); the default runs one whole engine per rank (replicas)")
@@ -576,13 +579,31 @@ def main_ours(a):
     K, W = max(1, a.steps), max(3, a.warmup)
     lanes = max(1, min(4, a.lanes))
     peaks, peak_src = measured_peaks()
-    int8_tops = int8_cublas_tops(torch) if rank == 0 else None
+    int8_tops = int8_cublas_tops(torch) if rank == 0 and not a.profile else None
     sampler = ClockSampler()
     if rank == 0:
         sampler.start()
 
     # ---- the headline configuration
     p = svc.params(a.rows, a.record_bytes)
+    if a.profile:
+        st, e = engine_for(svc, eng, p, host_db=False)
+        m = Measure(torch, e, p, a.batch, 1000 + rank, 1, barrier, world, sampler)
+        e.set_graphs(False)
+        for _ in range(max(1, a.warmup)):
+            m._enqueue(0)
+        e.sync()
+        for _ in range(a.profile):
+            m._enqueue(0)
+        e.sync()
+        for _ in range(a.profile):
+            assert e.answer_raw(m.req_ptrs, m.lens, a.batch, m.out_ptrs, m.h_status) == a.batch
+        sampler.stop()
+        m.close()
+        e.close()
+        print(f"profile: {a.profile} device batches and {a.profile} alto_answer calls of {a.batch} frames",
+              file=sys.stderr)
+        return 0
     want_cpu = rank == 0 and world == 1 and not a.no_cpu_baseline
     st, e = engine_for(svc, eng, p, host_db=want_cpu)
     m = Measure(torch, e, p, a.batch, 1000 + rank, lanes, barrier, world, sampler)

@@ -279,6 +279,18 @@ void alto_fill_bytes(uint8_t *dst, size_t count, uint64_t seed, int threads);
 void alto_synthetic_request(uint8_t *frame, size_t rows, size_t tg_n, uint64_t seed, uint64_t client);
 void alto_pack_encode(int8_t *ub, const uint32_t *U, size_t cols, size_t K, int threads);
 
+/* Offline hint on the device (row (f)1 of the offline set-up): the ring multiply of YServer::answer_hint_ring /
+ * multiply_with_db_ring (src/server.rs:656-768) over this engine's resident database, once per database.  query
+ * holds rows / n raw query polynomials of n coefficients (u64, reduced mod q here) -- the pseudorandom query of
+ * generate_pseudorandom_query (src/server.rs:714-738) before its preprocessing, which this call applies: polynomial
+ * r is negated and reversed as util.rs negacyclic_perm does (shift 0) and multiplied, modulo X^n + 1 and q, by the
+ * polynomial of records [r n, (r + 1) n) of each column.  out[z * cols + col] (n * cols u64 values < q, the layout
+ * answer_hint_ring returns) = coefficient z of the sum over r, passed once more through negacyclic_perm when
+ * perm_out != 0 (the reference does so for seed 0 outside SimplePIR mode, src/server.rs:699-705).  Needs rows a
+ * multiple of n and n a power of two <= 2048 (2n must divide q - 1).  Allocates its device scratch (about
+ * 8 n cols bytes) for the call.  0, -1 for bad arguments or an unsupported n, -4 for a device failure. */
+int alto_hint_ring(void *engine, const uint64_t *query, uint64_t *out, int perm_out);
+
 /* Self-check of the engine's modulus-switch arithmetic on the host: sum over v in [v0, v1) of rescale(v) * (2v + 1)
  * modulo 2^64, where rescale is the exact integer centred rescale Q -> q1 that the tail kernel runs. */
 uint64_t alto_rescale_digest(uint64_t q1, uint64_t v0, uint64_t v1, int threads);

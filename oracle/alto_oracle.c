@@ -342,3 +342,41 @@ void orc_pack_build(uint32_t *U, const uint64_t *const *bold_t, const uint64_t *
         free(col);
     }
 }
+
+/* ---------------------------------------------------------------- offline hint ring multiply (src/server.rs:656-768) */
+
+/* answer_hint_ring for columns [c0, c1) of a column-order database (db[col * ld + r], rows records, rows % n == 0),
+ * schoolbook: hint_col = sum over r < rows / n of perm(q_r) * D_{col,r} mod (X^n + 1, Q), where perm is util.rs
+ * negacyclic_perm with shift 0 (perm(a)_0 = a_0, perm(a)_i = -a_{n-i}; the preprocessing of
+ * generate_pseudorandom_query, src/server.rs:724-733) and D_{col,r} the polynomial of records [r n, (r + 1) n).  The
+ * reference multiplies in the NTT domain and keeps the coefficient-domain sum (src/server.rs:674-697); with
+ * perm_out the sum passes through negacyclic_perm once more (src/server.rs:699-705).  out[z * ostride + (col - c0)]. */
+void orc_hint_ring(uint64_t *out, size_t ostride, const uint8_t *db, size_t ld, size_t rows, size_t c0, size_t c1,
+                   const uint64_t *query, size_t n, int perm_out) {
+    const size_t polys = rows / n;
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (size_t col = c0; col < c1; col++) {
+        uint64_t *pos = (uint64_t *)calloc(n, sizeof(uint64_t)), *neg = (uint64_t *)calloc(n, sizeof(uint64_t));
+        uint64_t *a = (uint64_t *)malloc(n * sizeof(uint64_t));
+        for (size_t p = 0; p < polys; p++) {
+            const uint64_t *q = query + p * n;
+            a[0] = q[0] % ORC_Q;
+            for (size_t i = 1; i < n; i++) a[i] = (ORC_Q - q[n - i] % ORC_Q) % ORC_Q;
+            const uint8_t *d = db + col * ld + p * n;
+            for (size_t i = 0; i < n; i++) {
+                for (size_t j = 0; j < n; j++) {
+                    const uint64_t t = a[i] * d[j];           /* < 2^40 */
+                    if (i + j < n) pos[i + j] += t; else neg[i + j - n] += t;  /* X^n = -1 */
+                }
+            }
+            for (size_t k = 0; k < n; k++) { pos[k] %= ORC_Q; neg[k] %= ORC_Q; }  /* sums stay below 2^64 */
+        }
+        for (size_t z = 0; z < n; z++) {
+            const size_t src = perm_out && z ? n - z : z;
+            uint64_t v = (pos[src] + ORC_Q - neg[src]) % ORC_Q;
+            if (perm_out && z) v = (ORC_Q - v) % ORC_Q;
+            out[z * ostride + (col - c0)] = v;
+        }
+        free(pos); free(neg); free(a);
+    }
+}

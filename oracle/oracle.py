@@ -108,6 +108,7 @@ class Oracle:
             ("orc_fill_uniform_u64", None, [P, S, U64, U64]),
             ("orc_fill_bytes", None, [P, S, U64]),
             ("orc_synthetic_request", None, [P, S, S, U64, U64]),
+            ("orc_hint_ring", None, [P, S, P, S, S, S, S, P, S, I]),
         ]:
             f = getattr(L, name)
             f.restype, f.argtypes = res, args
@@ -219,6 +220,15 @@ class Oracle:
     def fill_bytes(self, count, seed):
         out = np.empty(count, dtype=np.uint8)
         self.L.orc_fill_bytes(_p(out), count, seed)
+        return out
+
+    def hint_ring(self, db_col, query, n, c0, c1, perm_out=False):
+        """The offline hint's ring multiply (orc_hint_ring) for columns [c0, c1) of a column-order database:
+        an (n, c1 - c0) uint64 array."""
+        q = np.ascontiguousarray(query, dtype=np.uint64)
+        out = np.empty((n, c1 - c0), dtype=np.uint64)
+        self.L.orc_hint_ring(_p(out), c1 - c0, _p(db_col), db_col.shape[1], db_col.shape[1], c0, c1, _p(q), n,
+                             int(perm_out))
         return out
 
     def synthetic_requests(self, p, b, seed, first_client=0):

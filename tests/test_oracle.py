@@ -179,3 +179,41 @@ def test_oracle_state_and_frames_equal_the_engine_generators(oracle, svc):
         assert np.array_equal(so.inv_table, st.inv_table)
         assert np.array_equal(oracle.synthetic_requests(po, 3, seed=1000, first_client=2),
                               svc.synthetic_requests(p, 3, seed=1000, first_client=2))
+
+
+def test_oracle_hint_ring_is_the_negacyclic_product_of_the_reference(oracle):
+    """orc_hint_ring against a direct restatement of src/server.rs:656-768 at toy sizes: each query polynomial goes
+    through util.rs negacyclic_perm (shift 0), is multiplied by the column's polynomial modulo X^n + 1 and Q, and the
+    products are summed over the column's polynomials (then negacyclic_perm again when perm_out)."""
+    Q = 4294955009
+    rng = np.random.default_rng(7)
+
+    def negacyclic_perm(a):  # util.rs:5-21, shift 0
+        n = len(a)
+        return [a[0] % Q] + [(Q - a[n - i] % Q) % Q for i in range(1, n)]
+
+    def mul(a, b):  # product modulo X^n + 1
+        n = len(a)
+        out = [0] * n
+        for i in range(n):
+            for j in range(n):
+                if i + j < n:
+                    out[i + j] += a[i] * b[j]
+                else:
+                    out[i + j - n] -= a[i] * b[j]
+        return [x % Q for x in out]
+
+    for n, rows, cols, perm_out in ((8, 32, 5, False), (16, 32, 3, True), (4, 4, 2, False)):
+        db = rng.integers(0, 256, (cols, rows), dtype=np.uint8)
+        query = rng.integers(0, 1 << 63, (rows // n, n), dtype=np.uint64)
+        want = np.zeros((n, cols), dtype=np.uint64)
+        for c in range(cols):
+            acc = [0] * n
+            for r in range(rows // n):
+                prod = mul(negacyclic_perm([int(x) for x in query[r]]), [int(x) for x in db[c, r * n:(r + 1) * n]])
+                acc = [(x + y) % Q for x, y in zip(acc, prod)]
+            if perm_out:
+                acc = negacyclic_perm(acc)
+            want[:, c] = acc
+        assert np.array_equal(oracle.hint_ring(db, query, n, 0, cols, perm_out), want), (n, rows, cols)
+        assert np.array_equal(oracle.hint_ring(db, query, n, 1, cols, perm_out), want[:, 1:])
