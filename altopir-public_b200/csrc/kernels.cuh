@@ -288,22 +288,40 @@ __global__ void __launch_bounds__((1 << L) / 8) tail_kernel(TailArgs a) {
       if (s0 + r < L) {
         for (int m = 0; m < 8; ++m) x[m] = y[m];
       } else {
-        // last round: modulus switch of these coefficients and their bits into the response part
-        for (int m = 0; m < (1 << r); ++m) {
-          const int i = tail_index<L>(oo, m, s0, r);
-          const uint32_t inter = (uint32_t)(((uint64_t)a.acc[base + i] * kQ + (1ull << 31)) >> 32);
-          const uint32_t t = rescale_q(add_q(inter, y[m]), (uint32_t)a.q1);
-          const uint32_t p = (uint32_t)a.row1_off + (uint32_t)i * (uint32_t)a.q1_bits;
-          const uint32_t sh = p & 31u;
-          atomicOr(&res[p >> 5], t << sh);
-          if (sh) {
-            const uint32_t hi = t >> (32u - sh);
-            if (hi) atomicOr(&res[(p >> 5) + 1], hi);
-          }
-        }
+        // last round: back into place (each location is read and written by this thread alone in this round)
+        for (int m = 0; m < (1 << r); ++m) acc[tail_swz(tail_index<L>(oo, m, s0, r))] = y[m];
       }
     }
-    if (s0 + r < L) __syncthreads();
+    __syncthreads();
+  }
+
+  // modulus switch of coefficients 8 tid .. 8 tid + 7 and their q1_bits-bit values, LSB first, into the response
+  // part from bit row1_off: one contiguous run of bits per thread, ORed into the words it covers (the run's first
+  // and last words are shared with the neighbouring threads)
+  {
+    const int i0 = 8 * tid;
+    const uint4 v0 = *reinterpret_cast<const uint4 *>(acc + tail_swz(i0));
+    const uint4 v1 = *reinterpret_cast<const uint4 *>(acc + tail_swz(i0) + 4);
+    const uint4 s0v = *reinterpret_cast<const uint4 *>(a.acc + base + i0);
+    const uint4 s1v = *reinterpret_cast<const uint4 *>(a.acc + base + i0 + 4);
+    const uint32_t v[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+    const uint32_t sc[8] = {s0v.x, s0v.y, s0v.z, s0v.w, s1v.x, s1v.y, s1v.z, s1v.w};
+    const uint32_t qb = (uint32_t)a.q1_bits, p0 = (uint32_t)a.row1_off + (uint32_t)i0 * qb;
+    uint32_t word = p0 >> 5, fill = p0 & 31u;
+    uint64_t win = 0;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const uint32_t inter = (uint32_t)(((uint64_t)sc[m] * kQ + (1ull << 31)) >> 32);
+      win |= (uint64_t)rescale_q(add_q(inter, v[m]), (uint32_t)a.q1) << fill;
+      fill += qb;
+      if (fill >= 32) {
+        if ((uint32_t)win) atomicOr(&res[word], (uint32_t)win);
+        win >>= 32;
+        fill -= 32;
+        ++word;
+      }
+    }
+    if (fill && (uint32_t)win) atomicOr(&res[word], (uint32_t)win);
   }
   __syncthreads();
 

@@ -83,6 +83,7 @@ struct ServeSlot {
   std::vector<int> res;  // resident-table entry per frame (-1 none), in batch order
   std::vector<uint8_t> admit;  // 1 when the frame's batch admits its entry
   int n_new = 0, taken = 0;
+  bool failed = false;  // the batch did not complete on the device: none of its admissions holds a row
   double t_dispatch = 0;
 };
 
@@ -253,7 +254,7 @@ void settle(Server *s, ServeSlot &sl) {
     Resident &x = s->res[r];
     --x.in_flight;
     if (sl.admit[i]) {
-      const bool ok = sl.b.h_status[i] == 0 && *sl.b.h_err == 0;
+      const bool ok = !sl.failed && sl.b.h_status[i] == 0;
       if (ok) {
         x.valid = true;
       } else {  // an invalid or failed admission frees its row again
@@ -342,6 +343,7 @@ void batcher_loop(Server *s) {
     ServeSlot &sl = s->slots[si];
     sl.t_dispatch = now_s();
     sl.taken = (int)ids.size();
+    sl.failed = false;
     sl.ids.clear();
     sl.tix.clear();
     sl.res.clear();
@@ -415,6 +417,7 @@ void batcher_loop(Server *s) {
         for (Ticket *t : sl.tix) finish_ticket(s, *t, -4);
         sl.ids.clear();
         sl.tix.clear();
+        sl.failed = true;
       }
       s->inflight.push_back(si);
     }
@@ -449,7 +452,9 @@ void completer_loop(Server *s) {
       if (*sl.b.h_err) {  // a kernel wait timed out: clear the word for the next batch of this context
         cudaMemsetAsync(sl.b.d_err, 0, sizeof(uint32_t), sl.b.st);
         cudaStreamSynchronize(sl.b.st);
+        *sl.b.h_err = 0;
       }
+      if (!ok) sl.failed = true;
     }
     // responses out of the context, outside the lock (a ticket's response is read only once it is done)
     std::vector<int> st(sl.ids.size());
