@@ -79,12 +79,13 @@ class Server:
             self.close()
 
 
-def poisson_load(server, frames, rate_qps, seconds, seed=1, clients=4):
+def poisson_load(server, frames, rate_qps, seconds, seed=1, clients=4, grace_s=120.0):
     """Open-loop load: arrival times drawn from a Poisson process of rate_qps over `seconds`, frames taken round
     robin from `frames`, submitted by `clients` threads at their due times; each thread then collects its tickets.
     Returns (results, offered, elapsed_s) with results[i] = (frame index, status, response, latency_s), where the
     latency is the loop's own time from submit to completion and elapsed_s runs from the first arrival to the last
-    completion."""
+    completion.  The whole run is bounded: tickets not complete `grace_s` after the last arrival are reported as
+    TIMEOUT instead of being waited for one by one."""
     rng = np.random.default_rng(seed)
     t = np.cumsum(rng.exponential(1.0 / rate_qps, size=int(rate_qps * seconds * 1.5) + 8))
     t = t[t < seconds]
@@ -103,11 +104,13 @@ def poisson_load(server, frames, rate_qps, seconds, seed=1, clients=4):
                     break
                 time.sleep(min(d, 0.002))
             mine.append((i, server.submit(frames[i % len(frames)])))
+        deadline = start + seconds + grace_s
         for i, ticket in mine:
             if ticket < 0:
                 results[i] = (i % len(frames), ticket, None, 0.0)
                 continue
-            st, resp, lat_ms = server.wait(ticket, with_latency=True)
+            left_ms = int(max(0.0, deadline - time.perf_counter()) * 1e3)
+            st, resp, lat_ms = server.wait(ticket, timeout_ms=left_ms, with_latency=True)
             results[i] = (i % len(frames), st, resp, lat_ms * 1e-3)
             done_at[k] = max(done_at[k], t_first + t[i] + lat_ms * 1e-3)
 
