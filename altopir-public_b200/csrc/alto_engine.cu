@@ -186,6 +186,7 @@ bool upload_tiled(uint8_t *dst, const uint8_t *src, size_t pitch, size_t nrows, 
 // reduction an int32 limb sum can take exactly, so a scan unit never spans more than one chunk.
 constexpr size_t kRecordChunk = 32768;
 constexpr int kMaxLanes = 4;  // batch contexts alto_enqueue_device can rotate through
+constexpr int kQueryGroups = 8;  // alto_answer: at most this many record-chunk groups of query words
 
 // ------------------------------------------------------------------------------------------- engine
 // The device resources of one batch in flight: its stream, per-batch scratch (grown on demand) and error word.
@@ -257,6 +258,8 @@ struct Engine {
   cudaStream_t st_copy = nullptr;
   // host pipeline of alto_answer: keys uploaded, pack done, statuses ready, each column group's tail done
   cudaEvent_t ev_pack = nullptr, ev_status = nullptr, ev_group[8] = {};
+  // alto_answer over several record chunks: each chunk group's query words uploaded, and split
+  cudaEvent_t ev_qgrp[kQueryGroups] = {}, ev_sgrp[kQueryGroups] = {};
   // per batch: a ring of kMarks timing marks, accumulated into kernel_ms when the stream is synchronised
   cudaEvent_t marks[kTimingSets][kMarks] = {};
   int mark_next = 0, last_set = 0;
@@ -430,6 +433,9 @@ void destroy(Engine *e) {
     if (ev) cudaEventDestroy(ev);
   for (cudaEvent_t ev : e->ev_group)
     if (ev) cudaEventDestroy(ev);
+  for (const cudaEvent_t *set : {e->ev_qgrp, e->ev_sgrp})
+    for (int k = 0; k < kQueryGroups; ++k)
+      if (set[k]) cudaEventDestroy(set[k]);
   if (e->st_copy) cudaStreamDestroy(e->st_copy);
   for (auto &set : e->marks)
     for (cudaEvent_t &ev : set)
@@ -623,9 +629,12 @@ Plan make_plan(const Engine *e, size_t slots) {
 
 // The scan GEMM (acc sums, pre-zeroed) and the pack GEMM (beta) for `slots` clients under plan p.
 bool launch_scan(const Engine *e, const Plan &p, const CUtensorMap &map_q, uint32_t *acc, size_t slots,
-                 cudaStream_t st, uint32_t *err, int m0 = 0, int mg = -1) {
-  // scan tiles [m0, m0 + mg) along the database columns (all of them by default)
+                 cudaStream_t st, uint32_t *err, int m0 = 0, int mg = -1, int kb_lo = 0, int kb_hi = -1) {
+  // scan tiles [m0, m0 + mg) along the database columns (all of them by default), reduction blocks [kb_lo, kb_hi)
+  // (all records by default; a range starts and ends on record-chunk boundaries, so units never straddle one)
   if (mg < 0) mg = p.scan_m;
+  if (kb_hi < 0) kb_hi = p.scan_kb;
+  const int splits = (kb_hi - kb_lo + p.scan_kb_per - 1) / p.scan_kb_per;
   // The query limbs are re-read by every unit of a K chunk; mark them evict-last only while the whole operand
   // (4 bytes per record and client) is a small part of the 126 MB L2, so stale chunks never crowd it out.
   const int keep_b = 4 * round_up(slots, 4) * e->rows <= (size_t(32) << 20);
@@ -634,8 +643,9 @@ bool launch_scan(const Engine *e, const Plan &p, const CUtensorMap &map_q, uint3
     g.num_m = mg;
     g.m_begin = m0;
     g.num_n = p.scan_n;
-    g.num_units = mg * p.scan_n * p.scan_split;
-    g.kb_total = p.scan_kb;
+    g.num_units = mg * p.scan_n * splits;
+    g.kb_total = kb_hi;
+    g.kb_begin = kb_lo;
     g.kb_per_unit = p.scan_kb_per;
     g.rows_a = (int)e->cols;
     g.clients = (int)slots;
@@ -651,7 +661,8 @@ bool launch_scan(const Engine *e, const Plan &p, const CUtensorMap &map_q, uint3
   g.num_m = mg;
   g.m_begin = m0;
   g.num_n = p.num_n;
-  g.kb_total = p.scan_kb;
+  g.kb_total = kb_hi;
+  g.kb_begin = kb_lo;
   g.kb_per_unit = p.scan_kb_per;
   g.rows_a = (int)e->cols;
   g.clients = (int)slots;
@@ -660,7 +671,7 @@ bool launch_scan(const Engine *e, const Plan &p, const CUtensorMap &map_q, uint3
   g.err = err;
   g.b_keep = keep_b;
   g.kb_chunk = p.kb_chunk;
-  return dispatch_gemm<alto::Epi::kScan>(p.bn, e->map_db, map_q, g, mg * p.num_n * p.scan_split, st);
+  return dispatch_gemm<alto::Epi::kScan>(p.bn, e->map_db, map_q, g, mg * p.num_n * splits, st);
 }
 
 bool launch_pack(const Engine *e, const Plan &p, const CUtensorMap &map_y, uint32_t *beta, size_t slots,
@@ -808,14 +819,14 @@ bool enqueue_query_split(const Engine *e, const Batch *bt, const uint8_t *d_slot
 bool enqueue_scan_tails(Engine *e, Batch *bt, const Plan &p, const CUtensorMap &map_q, const uint8_t *d_slots,
                         size_t slot_stride, size_t slots, uint8_t *resp, size_t resp_stride, const Groups &gr,
                         const cudaEvent_t *done, int *launches, cudaEvent_t before_last_tail = nullptr,
-                        cudaEvent_t last_tail_after = nullptr, int inline_from = 8) {
+                        cudaEvent_t last_tail_after = nullptr, int inline_from = 8, int kb_lo = 0) {
   cudaStream_t st = bt->st;
   bool forked = false;
   for (int g = 0; g < gr.count; ++g) {
     const int o0 = gr.bounds[g], parts = gr.bounds[g + 1] - o0;
-    const bool ok = gr.count == 1 ? launch_scan(e, p, map_q, bt->d_acc, slots, st, bt->d_err)
+    const bool ok = gr.count == 1 ? launch_scan(e, p, map_q, bt->d_acc, slots, st, bt->d_err, 0, -1, kb_lo)
                                   : launch_scan(e, p, map_q, bt->d_acc, slots, st, bt->d_err, o0 * gr.tiles_per_part,
-                                                parts * gr.tiles_per_part);
+                                                parts * gr.tiles_per_part, kb_lo);
     if (!ok) return false;
     const bool last = g + 1 == gr.count;
     cudaStream_t ts = (last || g >= inline_from) ? st : bt->side;
@@ -1095,14 +1106,28 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
     return -4;
   ALTO_H(cudaEventRecord(e->ev_keys, st));
   ALTO_H(cudaStreamWaitEvent(sc, e->ev_keys, 0));
-  // then the query words (the scan's input) and last the z keys, which only validation and the tails read
+  // then the query words (the scan's input) and last the z keys, which only validation and the tails read.  A
+  // database of several record chunks takes its query words chunk group by chunk group (at most 8 groups), each
+  // group's limb split and scan starting as soon as its words are in, so that the upload of the later chunks
+  // overlaps the scan of the earlier ones.
   const size_t zbytes = 4 * e->count, qoff = ybytes + zbytes;
-  if (!copy_runs(
-          nc, e->want - qoff, [&](size_t i) { return (const void *)(req[cand[i]] + qoff); },
-          [&](size_t i) { return (void *)(bt->d_req + i * e->slot_stride + kSlotLead + qoff); },
-          cudaMemcpyHostToDevice, sc))
-    return -4;
-  ALTO_H(cudaEventRecord(e->ev_queries, sc));
+  const bool piped = e->overlap && e->nchunks > 1;
+  const size_t gsz = piped ? (e->nchunks + kQueryGroups - 1) / kQueryGroups : e->nchunks;  // chunks per group
+  const int qgroups = (int)((e->nchunks + gsz - 1) / gsz);
+  auto group_rows = [&](int k, size_t *r0, size_t *r1) {
+    *r0 = (size_t)k * gsz * e->chunk;
+    *r1 = std::min(e->rows, (size_t)(k + 1) * gsz * e->chunk);
+  };
+  for (int k = 0; k < qgroups; ++k) {
+    size_t r0, r1;
+    group_rows(k, &r0, &r1);
+    if (!copy_runs(
+            nc, 4 * (r1 - r0), [&](size_t i) { return (const void *)(req[cand[i]] + qoff + 4 * r0); },
+            [&](size_t i) { return (void *)(bt->d_req + i * e->slot_stride + kSlotLead + qoff + 4 * r0); },
+            cudaMemcpyHostToDevice, sc))
+      return -4;
+    ALTO_H(cudaEventRecord(piped ? e->ev_qgrp[k] : e->ev_queries, sc));
+  }
   if (!copy_runs(
           nc, zbytes, [&](size_t i) { return (const void *)(req[cand[i]] + ybytes); },
           [&](size_t i) { return (void *)(bt->d_req + i * e->slot_stride + kSlotLead + ybytes); },
@@ -1126,10 +1151,26 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
   // status download once the z keys are: on the side stream beside the pack (on the batch's stream after the pack
   // without the overlap).  The scans wait for the split only; the last tail also waits for the statuses.
   cudaStream_t vs = e->overlap ? bt->side : st;
-  ALTO_H(cudaStreamWaitEvent(vs, e->ev_queries, 0));
-  if (!enqueue_query_split(e, bt, bt->d_req, e->slot_stride, nc, vs)) return -4;
-  ++launches;
-  if (e->overlap) ALTO_H(cudaEventRecord(bt->ev_qready, vs));
+  if (!piped) {
+    ALTO_H(cudaStreamWaitEvent(vs, e->ev_queries, 0));
+    if (!enqueue_query_split(e, bt, bt->d_req, e->slot_stride, nc, vs)) return -4;
+    ++launches;
+    if (e->overlap) ALTO_H(cudaEventRecord(bt->ev_qready, vs));
+  } else {
+    ALTO_H(cudaMemsetAsync(bt->d_acc, 0, nc * e->cols * sizeof(uint32_t), vs));
+    for (int k = 0; k < qgroups; ++k) {
+      size_t r0, r1;
+      group_rows(k, &r0, &r1);
+      ALTO_H(cudaStreamWaitEvent(vs, e->ev_qgrp[k], 0));
+      const size_t work = ((r1 - r0) / 16) * (size_t)bp;
+      alto::limb_split_kernel<<<(unsigned)((work + 255) / 256), 256, 0, vs>>>(
+          bt->d_req, e->slot_stride, kSlotLead + 9 + 8 * e->count + 4 * r0, (int)nc, bp, r1 - r0, e->chunk,
+          bt->d_qlimb + (r0 / e->chunk) * (4 * (size_t)bp * e->chunk));
+      ALTO_H(cudaGetLastError());
+      ++launches;
+      ALTO_H(cudaEventRecord(e->ev_sgrp[k], vs));
+    }
+  }
   ALTO_H(cudaStreamWaitEvent(vs, e->ev_zkeys, 0));
   alto::validate_kernel<<<(unsigned)nc, 256, 0, vs>>>(bt->d_req, e->slot_stride, kSlotLead, e->count, e->rows,
                                                       bt->d_status);
@@ -1137,9 +1178,26 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
   ++launches;
   ALTO_H(cudaMemcpyAsync(bt->h_status, bt->d_status, nc * sizeof(int), cudaMemcpyDeviceToHost, vs));
   ALTO_H(cudaEventRecord(e->ev_status, vs));
-  if (e->overlap) ALTO_H(cudaStreamWaitEvent(st, bt->ev_qready, 0));
+  int kb_last = 0;  // the scan in column groups (with the tails) covers the last chunk group
+  if (piped) {
+    for (int k = 0; k + 1 < qgroups; ++k) {  // every earlier chunk group, all columns, as soon as it is split
+      size_t r0, r1;
+      group_rows(k, &r0, &r1);
+      ALTO_H(cudaStreamWaitEvent(st, e->ev_sgrp[k], 0));
+      if (!launch_scan(e, p, map_q, bt->d_acc, nc, st, bt->d_err, 0, -1, (int)(r0 / alto::kBK),
+                       (int)((r1 + alto::kBK - 1) / alto::kBK)))
+        return -4;
+      ++launches;
+    }
+    size_t r0, r1;
+    group_rows(qgroups - 1, &r0, &r1);
+    ALTO_H(cudaStreamWaitEvent(st, e->ev_sgrp[qgroups - 1], 0));
+    kb_last = (int)(r0 / alto::kBK);
+  } else if (e->overlap) {
+    ALTO_H(cudaStreamWaitEvent(st, bt->ev_qready, 0));
+  }
   if (!enqueue_scan_tails(e, bt, p, map_q, bt->d_req, e->slot_stride, nc, bt->d_resp, e->resp_len, groups,
-                          e->ev_group, &launches, nullptr, e->ev_status, groups.count - e->host_inline - 1))
+                          e->ev_group, &launches, nullptr, e->ev_status, groups.count - e->host_inline - 1, kb_last))
     return -4;
   // the error word comes back behind the last tail, so the final synchronisation covers it
   ALTO_H(cudaMemcpyAsync(bt->h_err, bt->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
@@ -1302,6 +1360,9 @@ void *create_engine(const uint8_t *db_col, size_t ld, size_t rows, size_t cols, 
     return fail("event", err);
   for (cudaEvent_t &ev : e->ev_group)
     if ((err = cudaEventCreate(&ev)) != cudaSuccess) return fail("event", err);
+  for (cudaEvent_t *set : {e->ev_qgrp, e->ev_sgrp})
+    for (int k = 0; k < kQueryGroups; ++k)
+      if ((err = cudaEventCreateWithFlags(&set[k], cudaEventDisableTiming)) != cudaSuccess) return fail("event", err);
   for (auto &set : e->marks)
     for (cudaEvent_t &ev : set)
       if ((err = cudaEventCreate(&ev)) != cudaSuccess) return fail("event", err);

@@ -40,6 +40,8 @@ struct GemmArgs {
   int b_keep;       // 1: keep the B operand in L2 (evict_last; it is small and read by every unit), 0: normal
   int kb_chunk;     // scan: 128-byte blocks per record chunk of the 3-D query-limb map (units never straddle chunks)
   int m_begin;      // first tile along A (a launch may cover a column group: tiles m_begin .. m_begin + num_m)
+  int kb_begin = 0; // first 128-byte block of the reduction (a launch may cover a range of record chunks;
+                    // kb_total is then the range's end)
 };
 
 // x mod Q for any 64-bit x, using 2^32 = 12287 (mod Q): two folds leave x < 2^32 + 2^28, one subtraction finishes.
@@ -83,7 +85,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
   const int n_tile = u % args.num_n;
   const int m_tile = args.m_begin + (u / args.num_n) % args.num_m;
   const int k_chunk = u / (args.num_n * args.num_m);
-  const int kb0 = k_chunk * args.kb_per_unit;
+  const int kb0 = args.kb_begin + k_chunk * args.kb_per_unit;
   const int kb1 = min(kb0 + args.kb_per_unit, args.kb_total);
   const int nkb = kb1 - kb0;  // >= 1 by construction of the grid
 

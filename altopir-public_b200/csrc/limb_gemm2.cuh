@@ -54,6 +54,8 @@ struct PairArgs {
   int b_keep;       // 1: keep the B operand in L2 (evict_last; it is small and read by every unit), 0: normal
   int kb_chunk;     // scan: 128-byte blocks per record chunk of the 3-D query-limb map (units never straddle chunks)
   int m_begin;      // first 256-row tile along A (a launch may cover a column group)
+  int kb_begin = 0; // first 128-byte block of the reduction (a launch may cover a range of record chunks;
+                    // kb_total is then the range's end)
 };
 
 // Epilogue of 16 TMEM columns (4 clients x 4 limbs) for one accumulator row of the scan: row = database column.
@@ -140,7 +142,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
     n = u % args.num_n;
     m = args.m_begin + (u / args.num_n) % args.num_m;
     const int kc = u / (args.num_n * args.num_m);
-    kb0 = kc * args.kb_per_unit;
+    kb0 = args.kb_begin + kc * args.kb_per_unit;
     nkb = min(kb0 + args.kb_per_unit, args.kb_total) - kb0;
   };
 

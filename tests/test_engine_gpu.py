@@ -348,3 +348,34 @@ def test_batch_lanes_return_the_same_bytes(gpu, svc, eng):
     e.set_lanes(1)
     e.set_graphs(False)
     e.close()
+
+
+def test_answer_over_several_record_chunks_pipelines_the_upload(gpu, oracle, svc, eng):
+    """alto_answer over a database of six record chunks (the last one partial): the query words upload chunk group
+    by chunk group and each group's scan starts as soon as its words are split; the responses equal the device
+    path's (one scan over all records) and the oracle's."""
+    import torch
+    p = svc.Params(5 * 32768 + 8192, 4096)
+    st = svc.SyntheticState.make(p, seed=131, full_prefix=True)
+    e = eng.Engine.from_state(st)
+    b = 6
+    req = svc.synthetic_requests(p, b, seed=132)
+    req[2, 9:13] = 0xFF  # y[0] >= Q: status 3, no response
+    n, status, out = _answer(e, [req[i] for i in range(b)])
+    assert n == b - 1 and list(status) == [0, 0, 3, 0, 0, 0]
+    stride = (7 + e.request_len() + 15) // 16 * 16
+    slots = torch.zeros((b, stride), dtype=torch.uint8, device="cuda")
+    slots[:, 7:7 + e.request_len()] = torch.from_numpy(req).cuda()
+    d_out = torch.zeros((b, e.response_len()), dtype=torch.uint8, device="cuda")
+    dst = np.full(b, -1, dtype=np.int32)
+    torch.cuda.synchronize()
+    assert e.answer_device(slots.data_ptr(), stride, b, d_out.data_ptr(), e.response_len(), dst) == b - 1
+    dev = d_out.cpu().numpy()
+    ok = [c for c in range(b) if c != 2]
+    assert np.array_equal(dev[ok], out[ok])
+    part = st.prefixes[0].size
+    want = oracle.answer_parts(st, [req[c] for c in ok], [c % p.instances for c in ok])
+    for k, c in enumerate(ok):
+        o = c % p.instances
+        assert np.array_equal(out[c, o * part:(o + 1) * part], want[k]), c
+    e.close()
