@@ -553,6 +553,7 @@ int pick_bn(size_t limb_cols) {
 struct Plan {
   bool pair = false;  // CTA-pair kernels (limb columns > 16) or the single-CTA kernels
   bool wide = false;  // scan units of 512 limb columns (one read of each database tile for all of them)
+  bool pack_wide = false;  // pack units of 512 limb columns (one read of each packing-matrix tile for all of them)
   int scan_n = 1;     // scan tiles along the limb columns (num_n / 2 when wide)
   int kb_chunk = 1;   // scan blocks per record chunk
   int bn = 16, num_n = 1;
@@ -623,7 +624,11 @@ Plan make_plan(const Engine *e, size_t slots) {
   p.scan_kb_per = chunk_aligned((int)((p.scan_kb + split - 1) / split));
   p.scan_split = (p.scan_kb + p.scan_kb_per - 1) / p.scan_kb_per;
   p.pairs_scan = (int)std::min<long>(pairs, tiles * p.scan_split);
-  p.pairs_pack = (int)std::min<long>(pairs, (long)p.pack_m * p.num_n);
+  // Wide pack units (ALTO_PACK_WIDE=1): both 256-column tiles of the limb columns in one unit, so each packing-
+  // matrix tile is read once (and the epilogue no longer overlaps the next unit's MMAs)
+  if (const char *w = getenv("ALTO_PACK_WIDE")) p.pack_wide = p.bn == 256 && p.num_n >= 2 && w[0] == '1';
+  const long pack_n = p.pack_wide ? (p.num_n + 1) / 2 : p.num_n;
+  p.pairs_pack = (int)std::min<long>(pairs, (long)p.pack_m * pack_n);
   return p;
 }
 
@@ -681,8 +686,8 @@ bool launch_pack(const Engine *e, const Plan &p, const CUtensorMap &map_y, uint3
     alto::PairArgs g;
     g.num_m = p.pack_m;
     g.m_begin = 0;
-    g.num_n = p.num_n;
-    g.num_units = p.pack_m * p.num_n;
+    g.num_n = p.pack_wide ? (p.num_n + 1) / 2 : p.num_n;
+    g.num_units = p.pack_m * g.num_n;
     g.kb_total = p.pack_kb;
     g.kb_per_unit = p.pack_kb;
     g.rows_a = (int)(4 * e->cols);
@@ -692,7 +697,7 @@ bool launch_pack(const Engine *e, const Plan &p, const CUtensorMap &map_y, uint3
     g.err = err;
     g.b_keep = keep_b;
     g.kb_chunk = 1;
-    return dispatch_pair<alto::Epi::kPack>(p.bn, e->map_ub, map_y, g, p.pairs_pack, st);
+    return dispatch_pair<alto::Epi::kPack>(p.bn, e->map_ub, map_y, g, p.pairs_pack, st, p.pack_wide);
   }
   alto::GemmArgs g;
   g.num_m = p.pack_m;

@@ -207,8 +207,10 @@ __device__ __forceinline__ void tail_round(uint32_t *x, int o, int s0, int r, co
   }
 }
 
-template <int L>
-__global__ void __launch_bounds__((1 << L) / 8) tail_kernel(TailArgs a) {
+// MINB: CTAs per SM the register budget is sized for (__launch_bounds__): at n = 2048 a batch of 128 clients and 8
+// parts is 1024 CTAs, so the register count decides between one wave and one and a fraction.
+template <int L, int MINB>
+__global__ void __launch_bounds__((1 << L) / 8, MINB) tail_kernel(TailArgs a) {
   constexpr int n = 1 << L, NT = n / 8;
   extern __shared__ uint32_t tsm[];
   const int slot = blockIdx.x / a.o_count, o = a.o_begin + blockIdx.x % a.o_count;
@@ -497,6 +499,8 @@ __global__ void synthetic_requests_kernel(uint8_t *slots, size_t stride, size_t 
 
 namespace alto {
 
+constexpr int kTailMinBlocks = 6;  // default register budget of the n = 2048 tail: 40 registers, 6 CTAs per SM
+
 // Launches the tail for `slots` frames on stream st: the radix-8 kernel for n >= 256, the simple one below.
 inline cudaError_t launch_tail(const TailArgs &t, size_t slots, cudaStream_t st) {
   const size_t smem = ((size_t)t.n + (t.part_len + 3) / 4 + 1) * sizeof(uint32_t);
@@ -509,12 +513,22 @@ inline cudaError_t launch_tail(const TailArgs &t, size_t slots, cudaStream_t st)
       err = cudaGetLastError();
     }
   };
+  // ALTO_TAIL_MINB = 1, 6 or 8 picks the register budget of the n = 2048 tail (a tuning knob; same results)
+  static const int minb = [] {
+    const char *v = getenv("ALTO_TAIL_MINB");
+    const int m = v ? atoi(v) : kTailMinBlocks;
+    return (m == 1 || m == 6 || m == 8) ? m : kTailMinBlocks;
+  }();
   switch (t.n) {
-    case 256: go(tail_kernel<8>, 32); break;
-    case 512: go(tail_kernel<9>, 64); break;
-    case 1024: go(tail_kernel<10>, 128); break;
-    case 2048: go(tail_kernel<11>, 256); break;
-    case 4096: go(tail_kernel<12>, 512); break;
+    case 256: go(tail_kernel<8, 1>, 32); break;
+    case 512: go(tail_kernel<9, 1>, 64); break;
+    case 1024: go(tail_kernel<10, 1>, 128); break;
+    case 2048:
+      if (minb == 8) go(tail_kernel<11, 8>, 256);
+      else if (minb == 6) go(tail_kernel<11, 6>, 256);
+      else go(tail_kernel<11, 1>, 256);
+      break;
+    case 4096: go(tail_kernel<12, 1>, 512); break;
     default: go(tail_small_kernel, 128); break;
   }
   return err;

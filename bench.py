@@ -212,6 +212,31 @@ def int8_cublas_tops(torch):
         return None
 
 
+def int8_cublas_pack_shape(torch, count, cols, batch, min_s=1.0):
+    """cuBLASLt's int8 GEMM (torch._int_mm) of the pack's shape -- (4 cols) x (tg n) packing-matrix planes times
+    (tg n) x (4 batch) key limbs -- back to back for at least min_s, as the GEMMs of the timed region run: the library
+    rate under the same power cap (context for the roofline; its int32 output is not reduced mod Q)."""
+    try:
+        a = torch.randint(-128, 127, (4 * cols, count), dtype=torch.int8, device="cuda")
+        b = torch.randint(-128, 127, (count, 4 * batch), dtype=torch.int8, device="cuda")
+        for _ in range(3):
+            torch._int_mm(a, b)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n, ms = 0, 0.0
+        while ms < min_s * 1e3:
+            s.record()
+            for _ in range(20):
+                torch._int_mm(a, b)
+            e.record()
+            e.synchronize()
+            ms += s.elapsed_time(e)
+            n += 20
+        del a, b
+        return {"tops": 2.0 * 4 * cols * count * 4 * batch * n / (ms * 1e-3) / 1e12, "ms": ms / n, "launches": n}
+    except Exception as ex:  # noqa: BLE001 -- informational only
+        return {"error": str(ex)[:200]}
+
+
 def traffic_from_profile(kernel, rows, record_bytes, batch):
     """DRAM bytes per batch of `kernel` from the committed ncu capture (profiles/ncu_traffic.json): a one-kernel
     capture on a smaller database, scaled to this configuration where the file says how; None when it covers
@@ -629,6 +654,8 @@ def main_ours(a):
             exact_vs_ref = bool(np.array_equal(ref_out, dev[3]))
     st = None
 
+    cublas_pack = int8_cublas_pack_shape(torch, p.count, p.record_bytes, a.batch) if rank == 0 else None
+
     # ---- the larger databases (rank 0 of a one-GPU run): blocks of up to K steps, about 0.2 s each
     configs = []
     if world == 1 and not a.no_configs:
@@ -676,7 +703,8 @@ def main_ours(a):
                    "(alto_engine_set_lanes; consecutive batches overlap on the device), launch sequence replayed as "
                    "a CUDA graph; kernels and roofline from a second pass of the same batches launched directly on "
                    "one context",
-            "roofline": dict(res["roofline"], int8_cublaslt_tops=int8_tops),
+            "roofline": dict(res["roofline"], int8_cublaslt_tops=int8_tops,
+                             int8_cublaslt_pack_shape_sustained=cublas_pack),
             "kernels": res["kernels"], "cpu_baseline": cpu_baseline, "clocks": clocks,
             "plain_per_query": res["plain_per_query"],
             "byte_exact": dict(res["byte_exact"], vs_reference_engine=exact_vs_ref),

@@ -379,3 +379,31 @@ def test_answer_over_several_record_chunks_pipelines_the_upload(gpu, oracle, svc
         o = c % p.instances
         assert np.array_equal(out[c, o * part:(o + 1) * part], want[k]), c
     e.close()
+
+
+def test_wide_pack_units_return_identical_bytes(gpu, svc, eng, monkeypatch):
+    """ALTO_PACK_WIDE=1: pack units of 512 limb columns (two 256-column sub-accumulators over one read of each
+    packing-matrix tile), for an even and an odd count of 256-column tiles, on the host and device paths."""
+    import torch
+    p = svc.params(2048, 8192)
+    st = svc.SyntheticState.make(p, seed=141)
+    e = eng.Engine.from_state(st)
+    ql, rl = e.request_len(), e.response_len()
+    for b in (128, 136):
+        frames = svc.synthetic_requests(p, b, seed=142)
+        monkeypatch.delenv("ALTO_PACK_WIDE", raising=False)
+        n, status, want = _answer(e, [frames[i] for i in range(b)])
+        assert n == b
+        monkeypatch.setenv("ALTO_PACK_WIDE", "1")
+        n, status, got = _answer(e, [frames[i] for i in range(b)])
+        assert n == b and np.array_equal(got, want), b
+        stride = (7 + ql + 15) // 16 * 16
+        slots = torch.zeros((b, stride), dtype=torch.uint8, device="cuda")
+        slots[:, 7:7 + ql] = torch.from_numpy(frames).cuda()
+        out = torch.zeros((b, rl), dtype=torch.uint8, device="cuda")
+        dst = np.full(b, -1, dtype=np.int32)
+        torch.cuda.synchronize()
+        assert e.answer_device(slots.data_ptr(), stride, b, out.data_ptr(), rl, dst) == b
+        assert np.array_equal(out.cpu().numpy(), want), b
+    monkeypatch.delenv("ALTO_PACK_WIDE", raising=False)
+    e.close()
