@@ -78,6 +78,7 @@ struct ServeSlot {
   uint8_t *h_out = nullptr;  // pinned responses of the batch
   int *h_rows = nullptr, *d_rows = nullptr;  // per frame: table row to gather from (resident) or store into, or -1
   cudaEvent_t done = nullptr, ev0 = nullptr, ev_up = nullptr, ev_pack = nullptr;
+  cudaEvent_t ev_valid = nullptr, ev_sgrp[kQueryGroups] = {};  // validation done; each query chunk group split
   std::vector<long long> ids;  // tickets on the device, in batch order
   std::vector<Ticket *> tix;
   std::vector<int> res;  // resident-table entry per frame (-1 none), in batch order
@@ -185,9 +186,15 @@ bool enqueue_serving(Server *s, ServeSlot &sl, size_t nc) {
   const size_t n_new = (size_t)sl.n_new;
   int launches = 0;
   ALTO_CK(cudaEventRecord(sl.ev0, st));
-  // frames from the pool into the staging slots, rows of the table per frame
+  // A database of several record chunks: the headers and keys upload first, then the query words chunk group by
+  // chunk group on the side stream, each group split as soon as it is in, and each group's scan starts once its
+  // split is done (as alto_answer does), so that the upload of the later chunks overlaps the scan of the earlier
+  // ones.  Otherwise the whole frames upload at once.
+  const bool piped = e->nchunks > 1;
+  const size_t qoff = 9 + 8 * e->count;
+  auto pool_at = [&](size_t i) { return s->pool + (size_t)sl.tix[i]->pool * s->pitch; };
   if (!copy_runs(
-          nc, s->want, [&](size_t i) { return (const void *)(s->pool + (size_t)sl.tix[i]->pool * s->pitch); },
+          nc, piped ? qoff : s->want, [&](size_t i) { return (const void *)pool_at(i); },
           [&](size_t i) { return (void *)(bt->d_req + i * e->slot_stride + kSlotLead); }, cudaMemcpyHostToDevice, st))
     return false;
   ALTO_CK(cudaMemcpyAsync(sl.d_rows, sl.h_rows, nc * sizeof(int), cudaMemcpyHostToDevice, st));
@@ -200,9 +207,37 @@ bool enqueue_serving(Server *s, ServeSlot &sl, size_t nc) {
   ALTO_CK(cudaGetLastError());
   ++launches;
   ALTO_CK(cudaMemcpyAsync(bt->h_status, bt->d_status, nc * sizeof(int), cudaMemcpyDeviceToHost, vs));
-  if (!enqueue_query_split(e, bt, bt->d_req, e->slot_stride, nc, vs)) return false;
-  ++launches;
-  ALTO_CK(cudaEventRecord(bt->ev_qready, vs));
+  ALTO_CK(cudaEventRecord(sl.ev_valid, vs));
+  const size_t gsz = (e->nchunks + kQueryGroups - 1) / kQueryGroups;  // chunks per group
+  const int qgroups = piped ? (int)((e->nchunks + gsz - 1) / gsz) : 1;
+  auto group_rows = [&](int k, size_t *r0, size_t *r1) {
+    *r0 = (size_t)k * gsz * e->chunk;
+    *r1 = std::min(e->rows, (size_t)(k + 1) * gsz * e->chunk);
+  };
+  const int bq = (int)round_up(nc, 4);
+  if (!piped) {
+    if (!enqueue_query_split(e, bt, bt->d_req, e->slot_stride, nc, vs)) return false;
+    ++launches;
+    ALTO_CK(cudaEventRecord(bt->ev_qready, vs));
+  } else {
+    ALTO_CK(cudaMemsetAsync(bt->d_acc, 0, nc * e->cols * sizeof(uint32_t), vs));
+    for (int k = 0; k < qgroups; ++k) {
+      size_t r0, r1;
+      group_rows(k, &r0, &r1);
+      if (!copy_runs(
+              nc, 4 * (r1 - r0), [&](size_t i) { return (const void *)(pool_at(i) + qoff + 4 * r0); },
+              [&](size_t i) { return (void *)(bt->d_req + i * e->slot_stride + kSlotLead + qoff + 4 * r0); },
+              cudaMemcpyHostToDevice, vs))
+        return false;
+      const size_t work = ((r1 - r0) / 16) * (size_t)bq;
+      alto::limb_split_kernel<<<(unsigned)((work + 255) / 256), 256, 0, vs>>>(
+          bt->d_req, e->slot_stride, kSlotLead + qoff + 4 * r0, (int)nc, bq, r1 - r0, e->chunk,
+          bt->d_qlimb + (r0 / e->chunk) * (4 * (size_t)bq * e->chunk));
+      ALTO_CK(cudaGetLastError());
+      ++launches;
+      ALTO_CK(cudaEventRecord(sl.ev_sgrp[k], vs));
+    }
+  }
   const Plan ps = make_plan(e, nc);
   CUtensorMap map_q, map_y, unused;
   if (!make_limb_maps(e, ps, bt->d_qlimb, bt->d_ylimb, round_up(nc, 4), &map_q, &unused)) return false;
@@ -225,7 +260,7 @@ bool enqueue_serving(Server *s, ServeSlot &sl, size_t nc) {
     ++launches;
   }
   ALTO_CK(cudaEventRecord(sl.ev_pack, st));
-  ALTO_CK(cudaStreamWaitEvent(st, bt->ev_qready, 0));
+  ALTO_CK(cudaStreamWaitEvent(st, piped ? sl.ev_valid : bt->ev_qready, 0));
   bool store = false;
   for (size_t i = 0; i < n_new; ++i) store |= sl.admit[i] != 0;
   if (store) {  // after validation (joined above): only valid frames' rows are kept
@@ -234,9 +269,25 @@ bool enqueue_serving(Server *s, ServeSlot &sl, size_t nc) {
     ALTO_CK(cudaGetLastError());
     ++launches;
   }
+  int kb_last = 0;  // the scan in column groups (with the tails) covers the last chunk group
+  if (piped) {
+    for (int k = 0; k + 1 < qgroups; ++k) {
+      size_t r0, r1;
+      group_rows(k, &r0, &r1);
+      ALTO_CK(cudaStreamWaitEvent(st, sl.ev_sgrp[k], 0));
+      if (!launch_scan(e, ps, map_q, bt->d_acc, nc, st, bt->d_err, 0, -1, (int)(r0 / alto::kBK),
+                       (int)((r1 + alto::kBK - 1) / alto::kBK)))
+        return false;
+      ++launches;
+    }
+    size_t r0, r1;
+    group_rows(qgroups - 1, &r0, &r1);
+    ALTO_CK(cudaStreamWaitEvent(st, sl.ev_sgrp[qgroups - 1], 0));
+    kb_last = (int)(r0 / alto::kBK);
+  }
   const Groups groups = column_groups(e, ps, group_weights(e->overlap ? e->groups : 1, false));
   if (!enqueue_scan_tails(e, bt, ps, map_q, bt->d_req, e->slot_stride, nc, bt->d_resp, s->resp_len, groups, nullptr,
-                          &launches))
+                          &launches, nullptr, nullptr, 8, kb_last))
     return false;
   ALTO_CK(cudaMemcpyAsync(sl.h_out, bt->d_resp, nc * s->resp_len, cudaMemcpyDeviceToHost, st));
   ALTO_CK(cudaMemcpyAsync(bt->h_err, bt->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
@@ -512,6 +563,8 @@ bool server_start(Server *s, int nslots, size_t key_bytes) {
       ALTO_CK(cudaEventCreate(&sl.ev0));
       ALTO_CK(cudaEventCreate(&sl.ev_up));
       ALTO_CK(cudaEventCreate(&sl.ev_pack));
+      ALTO_CK(cudaEventCreateWithFlags(&sl.ev_valid, cudaEventDisableTiming));
+      for (cudaEvent_t &ev : sl.ev_sgrp) ALTO_CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
       ALTO_CK(cudaHostAlloc(&sl.h_out, s->max_batch * s->resp_len, cudaHostAllocDefault));
       ALTO_CK(cudaHostAlloc(&sl.h_rows, s->max_batch * sizeof(int), cudaHostAllocDefault));
       ALTO_CK(cudaMalloc(&sl.d_rows, s->max_batch * sizeof(int)));
@@ -537,7 +590,9 @@ void server_destroy(Server *s) {
   for (ServeSlot &sl : s->slots) {
     if (s->e) {
       destroy_batch(&sl.b);
-      for (cudaEvent_t ev : {sl.done, sl.ev0, sl.ev_up, sl.ev_pack})
+      for (cudaEvent_t ev : {sl.done, sl.ev0, sl.ev_up, sl.ev_pack, sl.ev_valid})
+        if (ev) cudaEventDestroy(ev);
+      for (cudaEvent_t ev : sl.ev_sgrp)
         if (ev) cudaEventDestroy(ev);
       cudaFreeHost(sl.h_out);
       cudaFreeHost(sl.h_rows);

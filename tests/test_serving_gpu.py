@@ -123,3 +123,36 @@ def test_resident_clients_skip_the_pack_and_answer_the_same(gpu, svc, eng):
             assert stats["table_rows"] == 0 and stats["resident_hits"] == 0 and stats["admitted"] == 0
         s.close()
     e.close()
+
+
+@pytest.mark.timeout(300, method="thread")
+def test_serving_over_several_record_chunks(gpu, svc, eng):
+    """A database of three record chunks (the last one partial): the loop uploads each batch's query words chunk
+    group by chunk group and starts each group's scan once it is split; every response equals the engine's answer
+    to the frame alone, with resident clients and a status-3 frame in the mix."""
+    from altopir_b200 import server as srv
+    p = svc.Params(2 * 32768 + 8192, 4096)
+    st = svc.SyntheticState.make(p, seed=151, full_prefix=True)
+    e = eng.Engine.from_state(st)
+    frames = [f for f in svc.synthetic_requests(p, 12, seed=152)]
+    frames[5] = frames[5].copy()
+    frames[5][9:13] = 0xFF  # y[0] >= Q: status 3
+    rl = e.response_len()
+    alone = []
+    for f in frames:
+        out = np.zeros((1, rl), dtype=np.uint8)
+        status = np.full(1, -1, dtype=np.int32)
+        e.answer([f], out, status)
+        alone.append((int(status[0]), out[0].copy()))
+    s = srv.Server(e, max_batch=8, queue_cap=64, slots=2)
+    for rnd in range(3):  # the second and third rounds find the valid clients resident
+        tickets = [(i, s.submit(frames[i])) for i in range(len(frames))]
+        for i, t in tickets:
+            code, resp = s.wait(t)
+            assert code == alone[i][0], (rnd, i)
+            if code == 0:
+                assert np.array_equal(resp, alone[i][1]), (rnd, i)
+    stats = s.stats()
+    assert stats["failed"] == 0 and stats["resident_hits"] > 0
+    s.close()
+    e.close()
