@@ -238,17 +238,15 @@ def int8_cublas_pack_shape(torch, count, cols, batch, min_s=1.0):
 
 
 def traffic_from_profile(kernel, rows, record_bytes, batch):
-    """DRAM bytes per batch of `kernel` from the committed ncu capture (profiles/ncu_traffic.json): a one-kernel
-    capture on a smaller database, scaled to this configuration where the file says how; None when it covers
-    neither."""
+    """DRAM bytes per batch of `kernel` (dram__bytes_read.sum + dram__bytes_write.sum over its launches in one batch)
+    from the committed ncu capture, profiles/ncu_traffic.json; None for a configuration it does not cover."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     try:
         with open(path) as f:
             d = json.load(f).get(kernel, {})
     except OSError:
         return None
-    per = d.get("scaled_to", {}).get(f"{rows}x{record_bytes}x{batch}")
-    return per if per is not None else None
+    return d.get("per_config", {}).get(f"{rows}x{record_bytes}x{batch}")
 
 
 # ------------------------------------------------------------------------------------------------ ranks
