@@ -272,14 +272,14 @@ struct Engine {
   bool overlap = true;      // the two-stream schedule of a batch (ALTO_OVERLAP=0 runs it on one stream)
   int groups = 2;           // column groups of the scan and tail of a device batch (ALTO_GROUPS: 1, 2, 4 or 8)
   // The column groups of alto_answer, whose downloads overlap the scan, as weights (ALTO_HOST_WEIGHTS, or
-  // ALTO_HOST_GROUPS groups with a last one of half the size).  A group's tail runs once the next group's scan has
-  // left the SMs, so the last two groups' tails and downloads follow the last scan.  At 1 GiB and B = 128, 2,2,2,1
-  // (5, 4, 5 and 2 of 16 parts) measured fastest with 6,4,3,2,1 (1.10 ms a call); 6,5,3,2, 5,5,4,2, 8,4,4, 8,4,2,2,
-  // 8,4,2,1,1 and 7,5,3,1 took 1.11-1.14 ms: what they save after the last scan, their smaller groups' scans cost.
-  std::vector<int> host_weights = {2, 2, 2, 1};
-  // alto_answer: the tails of this many groups before the last run on the batch's stream between their scan and the
-  // next group's, instead of beside the next scan (ALTO_HOST_INLINE)
-  int host_inline = 0;
+  // ALTO_HOST_GROUPS groups with a last one of half the size).  A group's side-stream tail runs once the next group's
+  // scan has left the SMs; the tails of the last host_inline groups before the last run on the batch's stream
+  // between their scan and the next (ALTO_HOST_INLINE), so that their downloads overlap that scan.  At 1 GiB and
+  // B = 128 under the power cap, six groups 3,3,2,2,1,1 with one in-line tail measured 1.104-1.109 ms a call against
+  // 1.134-1.136 for four groups 2,2,2,1 with none, 1.115-1.122 for 4,4,3,2,1 and 2,2,2,2 with one (three rounds,
+  // interleaved, same box).
+  std::vector<int> host_weights = {3, 3, 2, 2, 1, 1};
+  int host_inline = 1;
   std::vector<TuneEntry> tuning;  // sorted by b_max; the first entry with b_max >= batch size applies
 };
 
