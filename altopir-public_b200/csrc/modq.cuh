@@ -16,11 +16,14 @@ namespace alto {
 constexpr uint32_t kQ32 = 4294955009u;
 constexpr uint32_t kFold = 12287u;  // 2^32 mod Q
 
-// (a + b) mod Q.  On a carry the true sum a + b = s + 2^32 >= Q, and s - Q (mod 2^32) = s + 12287 is that sum
-// minus Q; without a carry one conditional subtraction suffices.
+ALTO_HD uint32_t umin_u32(uint32_t a, uint32_t b) { return a < b ? a : b; }
+
+// (a + b) mod Q.  d = s - Q (mod 2^32).  On a carry the true sum a + b = s + 2^32 >= Q, and d = s + 12287 is that
+// sum minus Q.  Without a carry, d < s exactly when s >= Q (below Q the subtraction wraps to s + 12287 > s), so the
+// smaller of s and d is the residue.
 ALTO_HD uint32_t add_q(uint32_t a, uint32_t b) {
-  const uint32_t s = a + b;
-  return (s < a || s >= kQ32) ? s - kQ32 : s;
+  const uint32_t s = a + b, d = s - kQ32;
+  return s < a ? d : umin_u32(s, d);
 }
 
 // (a - b) mod Q.
@@ -29,11 +32,14 @@ ALTO_HD uint32_t sub_q(uint32_t a, uint32_t b) {
   return a < b ? d + kQ32 : d;
 }
 
-// x mod Q for any 64-bit x: x = h 2^32 + l = 12287 h + l (mod Q); two folds leave x < 2^32 + 2^28.
+// x mod Q for any 64-bit x: x = h 2^32 + l = 12287 h + l (mod Q); two folds leave x < 2^32 + 2^28, whose high word
+// h is 0 or 1.  With h = 1, x - Q = l + 12287 < Q (l < 2^28); with h = 0 the smaller of l and l - Q (mod 2^32) is the
+// residue, as in add_q.
 ALTO_HD uint32_t red_q64(uint64_t x) {
   x = (x >> 32) * kFold + (x & 0xffffffffull);
   x = (x >> 32) * kFold + (x & 0xffffffffull);
-  return (uint32_t)(x >= kQ32 ? x - kQ32 : x);
+  const uint32_t t = (uint32_t)x + (uint32_t)(x >> 32) * kFold;
+  return umin_u32(t, t - kQ32);
 }
 
 // One fold of a 64-bit x: h 2^32 + l -> 12287 h + l, congruent to x mod Q and below 2^46 (not reduced).

@@ -50,3 +50,15 @@ def test_cpp_engine_answers_the_golden_case(gpu, golden, oracle, svc, host_api_b
     assert [sha(out[i]) for i in range(g["b"])] == g["sha256"]
     r, ost, oout = oracle.answer(st, [frames[i] for i in range(g["b"])])
     assert np.array_equal(out, oout)
+
+
+def test_modular_arithmetic_of_the_kernels(tmp_path):
+    """modq.cuh, the mod-Q helpers the tail kernels and the host share, against 128-bit arithmetic (edge values and
+    20 million seeded random cases per operation)."""
+    out = str(tmp_path / "test_modq")
+    res = subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Werror", os.path.join(ROOT, "tests", "cpp",
+                                                                                       "test_modq.cpp"), "-o", out],
+                         capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr
+    res = subprocess.run([out], capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0 and "OK" in res.stdout, res.stdout + res.stderr
