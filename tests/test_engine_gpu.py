@@ -407,3 +407,28 @@ def test_wide_pack_units_return_identical_bytes(gpu, svc, eng, monkeypatch):
         assert np.array_equal(out.cpu().numpy(), want), b
     monkeypatch.delenv("ALTO_PACK_WIDE", raising=False)
     e.close()
+
+
+def test_tail_register_budgets_return_identical_bytes(gpu, oracle, svc, eng):
+    """ALTO_TAIL_MINB (read once per process): the n = 2048 tail built for 1, 6 and 8 CTAs per SM answers the same
+    frames with the oracle's bytes; each budget runs in a process of its own."""
+    import os
+    import subprocess
+    import sys
+    from conftest import ROOT
+    code = (
+        "import sys, numpy as np; sys.path.insert(0, %r); sys.path.insert(0, %r)\n"
+        "import __graft_entry__ as ge; ge.load()\n"
+        "from altopir_b200 import engine as eng, service as svc\n"
+        "from oracle.oracle import Oracle\n"
+        "eng.init(); p = svc.params(2048, 4096); st = svc.SyntheticState.make(p, seed=161, full_prefix=True)\n"
+        "e = eng.Engine.from_state(st); f = svc.synthetic_requests(p, 9, seed=162)\n"
+        "out = np.zeros((9, e.response_len()), dtype=np.uint8); s = np.full(9, -1, dtype=np.int32)\n"
+        "assert e.answer([f[i] for i in range(9)], out, s)[0] == 9\n"
+        "r, _, want = Oracle().answer(st, [f[i] for i in range(9)])\n"
+        "assert np.array_equal(out, want); e.close(); print('OK')\n" % (ROOT, os.path.join(ROOT, "tests")))
+    for minb in ("1", "6", "8"):
+        env = dict(os.environ, ALTO_TAIL_MINB=minb)
+        res = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300, env=env,
+                             cwd=ROOT)
+        assert res.returncode == 0 and "OK" in res.stdout, (minb, res.stderr[-2000:])
