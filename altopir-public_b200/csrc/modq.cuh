@@ -71,12 +71,11 @@ ALTO_HD uint64_t div_q(uint64_t u) {
 ALTO_HD uint32_t rescale_q(uint32_t v, uint32_t q1) {
   constexpr uint64_t half = kQ32 / 2u;
   const bool neg = v >= (uint32_t)half;
-  const uint64_t mag = neg ? (uint64_t)(kQ32 - v) : (uint64_t)v;  // |c|
-  const uint64_t t = div_q(mag * q1 + half);                       // |trunc(x / Q)|, same sign as c
-  int64_t s = neg ? -(int64_t)t : (int64_t)t;
-  if (s < 0) s += q1;
-  if (s >= (int64_t)q1) s -= q1;
-  return (uint32_t)s;
+  const uint32_t mag = neg ? kQ32 - v : v;  // |c| <= ceil(Q / 2)
+  // |trunc(x / Q)| = floor((|c| q1 + floor(Q/2)) / Q) <= (q1 + 1) / 2 + 1: below q1 for every q1 >= 2, so a negative
+  // c maps to q1 - t (0 for t = 0) and a non-negative one to t
+  const uint32_t t = (uint32_t)div_q((uint64_t)mag * q1 + half);
+  return neg ? (t ? q1 - t : 0u) : (t >= q1 ? t - q1 : t);
 }
 
 }  // namespace alto
