@@ -187,6 +187,9 @@ bool upload_tiled(uint8_t *dst, const uint8_t *src, size_t pitch, size_t nrows, 
 constexpr size_t kRecordChunk = 32768;
 constexpr int kMaxLanes = 4;  // batch contexts alto_enqueue_device can rotate through
 constexpr int kQueryGroups = 8;  // alto_answer: at most this many record-chunk groups of query words
+// Batches whose query words are fewer bytes upload them at once: the upload is short against one scan launch, and
+// each extra scan launch ends on a partial round of its persistent CTA pairs.
+constexpr size_t kPipedQueryBytes = size_t(32) << 20;
 
 // ------------------------------------------------------------------------------------------- engine
 // The device resources of one batch in flight: its stream, per-batch scratch (grown on demand) and error word.
@@ -280,6 +283,9 @@ struct Engine {
   // interleaved, same box).
   std::vector<int> host_weights = {3, 3, 2, 2, 1, 1};
   int host_inline = 1;
+  // alto_answer and the serving loop upload a batch's query words by record-chunk group from this many bytes of
+  // query words on (ALTO_PIPED_BYTES)
+  size_t piped_bytes = kPipedQueryBytes;
   std::vector<TuneEntry> tuning;  // sorted by b_max; the first entry with b_max >= batch size applies
 };
 
@@ -1116,7 +1122,7 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
   // group's limb split and scan starting as soon as its words are in, so that the upload of the later chunks
   // overlaps the scan of the earlier ones.
   const size_t zbytes = 4 * e->count, qoff = ybytes + zbytes;
-  const bool piped = e->overlap && e->nchunks > 1;
+  const bool piped = e->overlap && e->nchunks > 1 && 4 * nc * e->rows >= e->piped_bytes;
   const size_t gsz = piped ? (e->nchunks + kQueryGroups - 1) / kQueryGroups : e->nchunks;  // chunks per group
   const int qgroups = (int)((e->nchunks + gsz - 1) / gsz);
   auto group_rows = [&](int k, size_t *r0, size_t *r1) {
@@ -1353,6 +1359,7 @@ void *create_engine(const uint8_t *db_col, size_t ld, size_t rows, size_t cols, 
   if (const char *v = getenv("ALTO_GROUPS")) e->groups = std::max(1, std::min(8, atoi(v)));
   if (const char *v = getenv("ALTO_HOST_GROUPS")) e->host_weights = group_weights(atoi(v), true);
   if (const char *v = getenv("ALTO_HOST_INLINE")) e->host_inline = std::max(0, std::min(7, atoi(v)));
+  if (const char *v = getenv("ALTO_PIPED_BYTES")) e->piped_bytes = (size_t)strtoull(v, nullptr, 10);
   if (const char *v = getenv("ALTO_HOST_WEIGHTS")) {
     std::vector<int> w = parse_weights(v);
     if (!w.empty()) e->host_weights = w;

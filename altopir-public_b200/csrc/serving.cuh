@@ -190,7 +190,7 @@ bool enqueue_serving(Server *s, ServeSlot &sl, size_t nc) {
   // chunk group on the side stream, each group split as soon as it is in, and each group's scan starts once its
   // split is done (as alto_answer does), so that the upload of the later chunks overlaps the scan of the earlier
   // ones.  Otherwise the whole frames upload at once.
-  const bool piped = e->nchunks > 1;
+  const bool piped = e->nchunks > 1 && 4 * nc * e->rows >= e->piped_bytes;
   const size_t qoff = 9 + 8 * e->count;
   auto pool_at = [&](size_t i) { return s->pool + (size_t)sl.tix[i]->pool * s->pitch; };
   if (!copy_runs(

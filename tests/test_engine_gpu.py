@@ -350,11 +350,14 @@ def test_batch_lanes_return_the_same_bytes(gpu, svc, eng):
     e.close()
 
 
-def test_answer_over_several_record_chunks_pipelines_the_upload(gpu, oracle, svc, eng):
-    """alto_answer over a database of six record chunks (the last one partial): the query words upload chunk group
-    by chunk group and each group's scan starts as soon as its words are split; the responses equal the device
+@pytest.mark.parametrize("piped_bytes", ["0", str(1 << 40)])
+def test_answer_over_several_record_chunks_pipelines_the_upload(gpu, oracle, svc, eng, monkeypatch, piped_bytes):
+    """alto_answer over a database of six record chunks (the last one partial): with ALTO_PIPED_BYTES=0 the query
+    words upload chunk group by chunk group and each group's scan starts as soon as its words are split (large
+    batches do so by default), with a threshold above the batch they upload at once; the responses equal the device
     path's (one scan over all records) and the oracle's."""
     import torch
+    monkeypatch.setenv("ALTO_PIPED_BYTES", piped_bytes)
     p = svc.Params(5 * 32768 + 8192, 4096)
     st = svc.SyntheticState.make(p, seed=131, full_prefix=True)
     e = eng.Engine.from_state(st)

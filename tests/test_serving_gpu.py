@@ -126,11 +126,12 @@ def test_resident_clients_skip_the_pack_and_answer_the_same(gpu, svc, eng):
 
 
 @pytest.mark.timeout(300, method="thread")
-def test_serving_over_several_record_chunks(gpu, svc, eng):
-    """A database of three record chunks (the last one partial): the loop uploads each batch's query words chunk
-    group by chunk group and starts each group's scan once it is split; every response equals the engine's answer
-    to the frame alone, with resident clients and a status-3 frame in the mix."""
+def test_serving_over_several_record_chunks(gpu, svc, eng, monkeypatch):
+    """A database of three record chunks (the last one partial), every batch pipelined (ALTO_PIPED_BYTES=0): the loop
+    uploads each batch's query words chunk group by chunk group and starts each group's scan once it is split; every
+    response equals the engine's answer to the frame alone, with resident clients and a status-3 frame in the mix."""
     from altopir_b200 import server as srv
+    monkeypatch.setenv("ALTO_PIPED_BYTES", "0")
     p = svc.Params(2 * 32768 + 8192, 4096)
     st = svc.SyntheticState.make(p, seed=151, full_prefix=True)
     e = eng.Engine.from_state(st)
