@@ -1189,9 +1189,14 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
   ++launches;
   ALTO_H(cudaMemcpyAsync(bt->h_status, bt->d_status, nc * sizeof(int), cudaMemcpyDeviceToHost, vs));
   ALTO_H(cudaEventRecord(e->ev_status, vs));
-  int kb_last = 0;  // the scan in column groups (with the tails) covers the last chunk group
+  // The scan in column groups (with the tails and downloads) covers the last quarter of the chunk groups, which it
+  // starts once all query words are in; the chunk groups before it scan all columns as they arrive.  The upload of
+  // the query words takes about three quarters of the scan's time (link bytes against int8 work per query word at
+  // 32 KB records), so by the time the last words are in, about that share of the scan is done.
+  const int qtail = qgroups - std::max(1, qgroups / 4);
+  int kb_last = 0;
   if (piped) {
-    for (int k = 0; k + 1 < qgroups; ++k) {  // every earlier chunk group, all columns, as soon as it is split
+    for (int k = 0; k < qtail; ++k) {  // every earlier chunk group, all columns, as soon as it is split
       size_t r0, r1;
       group_rows(k, &r0, &r1);
       ALTO_H(cudaStreamWaitEvent(st, e->ev_sgrp[k], 0));
@@ -1201,7 +1206,7 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
       ++launches;
     }
     size_t r0, r1;
-    group_rows(qgroups - 1, &r0, &r1);
+    group_rows(qtail, &r0, &r1);
     ALTO_H(cudaStreamWaitEvent(st, e->ev_sgrp[qgroups - 1], 0));
     kb_last = (int)(r0 / alto::kBK);
   } else if (e->overlap) {
