@@ -190,6 +190,9 @@ constexpr int kQueryGroups = 8;  // alto_answer: at most this many record-chunk 
 // Batches whose query words are fewer bytes upload them at once: the upload is short against one scan launch, and
 // each extra scan launch ends on a partial round of its persistent CTA pairs.
 constexpr size_t kPipedQueryBytes = size_t(32) << 20;
+// alto_answer splits the scan into column groups when a batch's responses are at least this many bytes (16 frames
+// of 32 KB records)
+constexpr size_t kGroupedRespBytes = size_t(2) << 20;
 
 // ------------------------------------------------------------------------------------------- engine
 // The device resources of one batch in flight: its stream, per-batch scratch (grown on demand) and error word.
@@ -1098,7 +1101,10 @@ int answer_host(Engine *e, const uint8_t *const *req, const size_t *len, size_t 
   cudaStream_t st = bt->st, sc = e->st_copy;
   const size_t nc = cand.size();
   const Plan p = make_plan(e, nc);
-  const Groups groups = column_groups(e, p, e->overlap ? e->host_weights : std::vector<int>{1});
+  // Column groups overlap the responses' download with the scan; a batch whose responses are few bytes has little to
+  // overlap, and every extra scan launch ends on a partial round of its CTA pairs, so it scans in one launch.
+  const bool grouped = e->overlap && nc * e->resp_len >= kGroupedRespBytes;
+  const Groups groups = column_groups(e, p, grouped ? e->host_weights : std::vector<int>{1});
   const int bp = (int)round_up(nc, 4);
   const size_t ybytes = 9 + 4 * e->count;  // header and y keys
   int launches = 0;
