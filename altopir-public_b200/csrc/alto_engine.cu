@@ -282,7 +282,7 @@ struct Engine {
   // scan has left the SMs; the tails of the last host_inline groups before the last run on the batch's stream
   // between their scan and the next (ALTO_HOST_INLINE), so that their downloads overlap that scan.  At 1 GiB and
   // B = 128 under the power cap, six groups 3,3,2,2,1,1 with one in-line tail measured 1.104-1.109 ms a call against
-  // 1.134-1.136 for four groups 2,2,2,1 with none, 1.115-1.122 for 4,4,3,2,1 and 2,2,2,2 with one (three rounds,
+  // 1.134-1.136 for four groups 2,2,2,1 with none, 1.115-1.122 for 4,4,3,2,1 and 2,2,2,2 with one (three repetitions,
   // interleaved, same box).
   std::vector<int> host_weights = {3, 3, 2, 2, 1, 1};
   int host_inline = 1;
