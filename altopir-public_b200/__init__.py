@@ -71,6 +71,7 @@ def _declare(L):
         "alto_synthetic_db_col_device": (I, [P, S, S, S, S]),
         "alto_engine_fill_synthetic": (I, [P]),
         "alto_hint_ring": (I, [P, P, P, I]),
+        "alto_engine_offline": (I, [P, P, P, P, P, P, P, P, c.POINTER(c.c_double)]),
         "alto_synthetic_requests_device": (I, [P, S, S, S, S, S, U64, U64]),
         "alto_fill_uniform_u32": (None, [P, S, U64, U64, I]),
         "alto_fill_uniform_u64": (None, [P, S, U64, U64, I]),
@@ -102,6 +103,7 @@ EXPORTS = (
     "alto_server_submit", "alto_server_wait", "alto_server_stats", "alto_server_free", "alto_engine_new_empty",
     "alto_engine_load_records", "alto_engine_load_file", "alto_synthetic_db_col", "alto_synthetic_db_col_device",
     "alto_engine_fill_synthetic", "alto_synthetic_requests_device", "alto_hint_ring",
+    "alto_engine_offline",
     "alto_fill_uniform_u32", "alto_fill_uniform_u64", "alto_fill_bytes", "alto_synthetic_request",
     "alto_pack_encode", "alto_rescale_digest",
 )

@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libaltopir_gpu.so")
 SOURCES = ["csrc/alto_engine.cu", "csrc/host_setup.cpp"]
 DEPS = SOURCES + ["csrc/kernels.cuh", "csrc/limb_gemm.cuh", "csrc/limb_gemm2.cuh", "csrc/sm100.cuh", "csrc/modq.cuh",
-                  "csrc/serving.cuh", "csrc/hint.cuh", "../include/altopir_gpu.h"]
+                  "csrc/serving.cuh", "csrc/hint.cuh", "csrc/offline.cuh", "../include/altopir_gpu.h"]
 
 
 def nvcc_path():

@@ -19,6 +19,7 @@
 #include "../../include/altopir_gpu.h"
 #include "hint.cuh"
 #include "kernels.cuh"
+#include "offline.cuh"
 #include "limb_gemm2.cuh"
 
 namespace {
@@ -1820,6 +1821,153 @@ int alto_hint_ring(void *p, const uint64_t *query, uint64_t *out, int perm_out) 
   cudaFree(d_out);
   if (err != cudaSuccess) {
     set_error("alto_hint_ring", err);
+    return -4;
+  }
+  return 0;
+}
+
+int alto_engine_offline(void *p, const uint64_t *query, const uint64_t *w_mask, const uint64_t *v_mask,
+                        uint32_t *bold_t, uint32_t *bold_t_bar, uint32_t *that, uint32_t *a_hat, double *ms) {
+  Engine *e = static_cast<Engine *>(p);
+  if (!e || !query || !w_mask || !v_mask) {
+    set_error("alto_engine_offline: bad arguments");
+    return -1;
+  }
+  const size_t n = e->n, tg = e->tg, cols = e->cols, outputs = e->outputs, half = n / 2;
+  std::vector<uint32_t> psi, psi_inv;
+  uint32_t n_inv = 0;
+  if (n < 8 || e->rows % n || e->row1_off % n || !alto::hint_tables((int)n, psi, psi_inv, n_inv)) {
+    set_error("alto_engine_offline: needs n a power of two in [8, 2048], records a multiple of n, row 1 at q2_bits n");
+    return -1;
+  }
+  const int q2_bits = (int)(e->row1_off / n);
+  if (q2_bits < 1 || q2_bits > 31 || ((size_t)q2_bits * n + 7) / 8 > e->part_len) {
+    set_error("alto_engine_offline: row 0 does not fit the response part");
+    return -1;
+  }
+  int logn = 0;
+  while ((size_t(1) << logn) < n) ++logn;
+  // gadget digits: floor(32 / t) + 1 bits each (one bit when t = 32), as get_bits_per gives for log2ceil(Q) = 32
+  const int bits = tg >= 32 ? 1 : (int)(32 / tg) + 1;
+  // dlog[(t - 1) / 2] = 2 i + bar for t = g^i (bar 0) or 2n - g^i (bar 1); inv_odd[x] = (2x + 1)^-1 mod 2n
+  std::vector<int16_t> dlog(n, -1);
+  std::vector<uint16_t> inv_odd(n);
+  for (size_t i = 0, g = 1; i < half; ++i, g = (g * 5) % (2 * n)) {
+    dlog[(g - 1) / 2] = (int16_t)(2 * i);
+    dlog[(2 * n - g - 1) / 2] = (int16_t)(2 * i + 1);
+  }
+  for (size_t x = 0; x < n; ++x) {
+    const size_t a = 2 * x + 1;
+    size_t inv = 1;  // the odd residues mod 2n form a group of order n, so a^(n - 1) = a^-1
+    for (size_t k = 0; k + 1 < n; ++k) inv = inv * a % (2 * n);
+    inv_odd[x] = (uint16_t)inv;
+  }
+  for (size_t x = 0; x < n; ++x)
+    if (dlog[x] < 0 || (2 * x + 1) * inv_odd[x] % (2 * n) != 1) {
+      set_error("alto_engine_offline: automorphism tables");
+      return -1;
+    }
+  if (cudaSetDevice(e->dev) != cudaSuccess) return -4;
+  for (int k = 0; k < e->lanes_made; ++k) {  // batches already enqueued read the packing state
+    if (cudaStreamSynchronize(lane_batch(e, k)->st) != cudaSuccess ||
+        cudaStreamSynchronize(lane_batch(e, k)->side) != cudaSuccess) {
+      set_error("alto_engine_offline", cudaGetLastError());
+      return -4;
+    }
+  }
+  std::vector<uint32_t> w32(tg * n), v32(tg * n);
+  for (size_t i = 0; i < tg * n; ++i) {
+    w32[i] = (uint32_t)(w_mask[i] % alto::kQ);
+    v32[i] = (uint32_t)(v_mask[i] % alto::kQ);
+  }
+  const size_t polys = e->rows / n, bt_words = outputs * 2 * (half - 1) * tg * n;
+  uint64_t *d_q = nullptr;
+  uint32_t *d_qhat = nullptr, *d_psi = nullptr, *d_psi_inv = nullptr, *d_w = nullptr, *d_v = nullptr;
+  uint32_t *d_act = nullptr, *d_bt = nullptr, *d_last = nullptr, *d_that = nullptr, *d_ahat = nullptr;
+  int16_t *d_dlog = nullptr;
+  uint16_t *d_inv_odd = nullptr;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  cudaError_t err = cudaSuccess;
+  auto step = [&](cudaError_t x) {
+    if (err == cudaSuccess) err = x;
+  };
+  step(cudaEventCreate(&t0));
+  step(cudaEventCreate(&t1));
+  step(cudaMalloc(&d_q, e->rows * sizeof(uint64_t)));
+  step(cudaMalloc(&d_qhat, e->rows * sizeof(uint32_t)));
+  step(cudaMalloc(&d_psi, n * sizeof(uint32_t)));
+  step(cudaMalloc(&d_psi_inv, n * sizeof(uint32_t)));
+  step(cudaMalloc(&d_w, tg * n * sizeof(uint32_t)));
+  step(cudaMalloc(&d_v, tg * n * sizeof(uint32_t)));
+  step(cudaMalloc(&d_act, cols * n * sizeof(uint32_t)));
+  step(cudaMalloc(&d_bt, bt_words * sizeof(uint32_t)));
+  step(cudaMalloc(&d_last, outputs * 2 * n * sizeof(uint32_t)));
+  step(cudaMalloc(&d_dlog, n * sizeof(int16_t)));
+  step(cudaMalloc(&d_inv_odd, n * sizeof(uint16_t)));
+  if (that) step(cudaMalloc(&d_that, outputs * tg * n * sizeof(uint32_t)));
+  if (a_hat) step(cudaMalloc(&d_ahat, outputs * n * sizeof(uint32_t)));
+  step(cudaMemcpy(d_q, query, e->rows * sizeof(uint64_t), cudaMemcpyHostToDevice));
+  step(cudaMemcpy(d_psi, psi.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  step(cudaMemcpy(d_psi_inv, psi_inv.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  step(cudaMemcpy(d_w, w32.data(), tg * n * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  step(cudaMemcpy(d_v, v32.data(), tg * n * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  step(cudaMemcpy(d_dlog, dlog.data(), n * sizeof(int16_t), cudaMemcpyHostToDevice));
+  step(cudaMemcpy(d_inv_odd, inv_odd.data(), n * sizeof(uint16_t), cudaMemcpyHostToDevice));
+  const size_t act_smem = (1 + alto::kActCols) * n * sizeof(uint32_t), walk_smem = (1 + tg) * n * sizeof(uint32_t);
+  step(cudaFuncSetAttribute(alto::offline_act_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)act_smem));
+  step(cudaFuncSetAttribute(alto::offline_walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)walk_smem));
+  step(cudaFuncSetAttribute(alto::offline_finish_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)walk_smem));
+  const unsigned nt = (unsigned)std::max<size_t>(32, std::min<size_t>(256, n / 2));
+  const unsigned wt = (unsigned)std::max<size_t>(64, std::min<size_t>(1024, tg * n / 2));
+  const uint32_t tail_scale = alto::inv_pow2_q(logn);
+  const size_t K = tg * n, planes_threads = cols * K;
+  if (err == cudaSuccess) {
+    step(cudaEventRecord(t0, 0));
+    // the hint's query: NTT(perm(q_p)), without the n^-1 the coefficient-domain hint folds in
+    alto::hint_query_kernel<<<(unsigned)polys, nt, n * sizeof(uint32_t)>>>(d_q, (int)n, d_psi, 1u, d_qhat);
+    step(cudaGetLastError());
+    alto::offline_act_kernel<<<(unsigned)(cols / alto::kActCols), 256, act_smem>>>(e->d_db, e->db_kbs, (int)n,
+                                                                                  (int)polys, d_qhat, d_psi, d_act);
+    step(cudaGetLastError());
+    alto::offline_rows_kernel<<<(unsigned)cols, nt, n * sizeof(uint32_t)>>>(d_act, (int)n, d_psi);
+    step(cudaGetLastError());
+    alto::offline_walk_kernel<<<(unsigned)(outputs * 2), wt, walk_smem>>>(d_act, (int)n, logn, (int)tg, bits, d_w,
+                                                                          d_psi, d_psi_inv, n_inv, d_bt, d_last);
+    step(cudaGetLastError());
+    alto::offline_finish_kernel<<<(unsigned)outputs, wt, walk_smem>>>(d_last, (int)n, (int)tg, bits, d_v, d_psi,
+                                                                      d_psi_inv, n_inv, tail_scale, e->d_that,
+                                                                      e->d_prefix, e->part_len, q2_bits, d_that, d_ahat);
+    step(cudaGetLastError());
+    alto::offline_planes_kernel<<<(unsigned)((planes_threads + 255) / 256), 256>>>(
+        d_bt, (int)n, logn, (int)tg, cols, d_dlog, d_inv_odd, tail_scale, e->d_ub, e->ub_kbs);
+    step(cudaGetLastError());
+    // the engine's tail twiddles: its inverse table psi^-brv / 2, doubled as create_engine stores it
+    step(cudaMemcpyAsync(e->d_tw, d_psi_inv, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, 0));
+    step(cudaEventRecord(t1, 0));
+    step(cudaEventSynchronize(t1));
+  }
+  if (err == cudaSuccess && ms) {
+    float f = 0.f;
+    step(cudaEventElapsedTime(&f, t0, t1));
+    *ms = f;
+  }
+  const size_t per = (half - 1) * tg * n;
+  for (size_t o = 0; o < outputs && err == cudaSuccess; ++o) {
+    if (bold_t)
+      step(cudaMemcpy(bold_t + o * per, d_bt + (o * 2) * per, per * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (bold_t_bar)
+      step(cudaMemcpy(bold_t_bar + o * per, d_bt + (o * 2 + 1) * per, per * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  }
+  if (that) step(cudaMemcpy(that, d_that, outputs * tg * n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  if (a_hat) step(cudaMemcpy(a_hat, d_ahat, outputs * n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  for (void *x : {(void *)d_q, (void *)d_qhat, (void *)d_psi, (void *)d_psi_inv, (void *)d_w, (void *)d_v,
+                  (void *)d_act, (void *)d_bt, (void *)d_last, (void *)d_dlog, (void *)d_inv_odd, (void *)d_that,
+                  (void *)d_ahat})
+    cudaFree(x);
+  if (t0) cudaEventDestroy(t0);
+  if (t1) cudaEventDestroy(t1);
+  if (err != cudaSuccess) {
+    set_error("alto_engine_offline", err);
     return -4;
   }
   return 0;

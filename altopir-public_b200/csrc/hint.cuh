@@ -87,8 +87,8 @@ __global__ void hint_ring_kernel(const uint8_t *__restrict__ db, size_t kbs, int
   }
 }
 
-// Host: a primitive 2n-th root of unity mod Q (2n must divide Q - 1 = 2^12 * 1048573, so n <= 2048) and the
-// transform tables psi[k] = psi^brv(k), psi_inv[k] = psi^-brv(k) (brv = bit reversal of log2 n bits).
+// Host: the smallest primitive 2n-th root of unity psi mod Q (2n must divide Q - 1 = 2^12 * 1048573, so n <= 2048)
+// and the transform tables psi[k] = psi^brv(k), psi_inv[k] = psi^-brv(k) (brv = bit reversal of log2 n bits).
 inline bool hint_tables(int n, std::vector<uint32_t> &psi, std::vector<uint32_t> &psi_inv, uint32_t &n_inv) {
   if (n < 2 || (n & (n - 1)) || (uint64_t)(kQ32 - 1) % (2 * (uint64_t)n)) return false;
   auto pow_q = [](uint32_t b, uint64_t e) {
@@ -100,12 +100,19 @@ inline bool hint_tables(int n, std::vector<uint32_t> &psi, std::vector<uint32_t>
     }
     return r;
   };
-  uint32_t root = 0;
-  for (uint32_t g = 2; g < 1000 && !root; ++g) {
+  uint32_t any = 0;
+  for (uint32_t g = 2; g < 1000 && !any; ++g) {
     const uint32_t c = pow_q(g, (kQ32 - 1) / (2 * (uint64_t)n));
-    if (pow_q(c, (uint64_t)n) == kQ32 - 1) root = c;  // order exactly 2n
+    if (pow_q(c, (uint64_t)n) == kQ32 - 1) any = c;  // order exactly 2n
   }
-  if (!root) return false;
+  if (!any) return false;
+  // the smallest primitive 2n-th root: the odd powers of any one are all of them
+  uint32_t root = any, x = any;
+  const uint32_t sq = mul_q(any, any);
+  for (int k = 3; k < 2 * n; k += 2) {
+    x = mul_q(x, sq);
+    root = x < root ? x : root;
+  }
   const uint32_t root_inv = pow_q(root, kQ32 - 2);
   int logn = 0;
   while ((1 << logn) < n) ++logn;

@@ -1,0 +1,240 @@
+// offline.cuh -- the scheme's offline set-up on the device, for an engine whose database is resident: the hint's
+// ring multiply kept in NTT form, the InspiRING precomputation of every output, the packing matrix, bold_t_hat and
+// the row-0 prefixes (Prepared::new, src/service.rs:127-157; YServer::perform_offline_precomputation_simplepir,
+// src/server.rs:947-1021; full_packing_with_preprocessing_offline, src/packing.rs:2260-2359).
+//
+// Ring Z_Q[X]/(X^n + 1).  NTT form: slot s holds the evaluation at psi^(2 brv(s) + 1) (Longa-Naehrig transforms of
+// hint.cuh over the tables psi^brv, psi^-brv), the slot order of the reference's automorphism tables, under which
+// tau_t acts as the permutation table_t[s] = brv(((t (2 brv(s) + 1)) mod 2n - 1) / 2).
+//
+// Per output o (n database columns, n = 2048 in the scheme) the reference computes
+//   act[j]  = NTT(perm(hint column o n + j))                       prep_pack_lwes (src/packing.rs:910-942)
+//   ev[v]   = NTT over j of act[j][v]                               precompute_aggregates_ntt (:2260-2291)
+//   r_i     = n^-1 ev[table_(g^i)[s]][s],  rbar_i the same with 2n - g^i,  g = 5, i < n / 2
+//   walk i = n/2 - 2 .. 0:  bold_t[i] = NTT(G^-1(r_(i+1))),  r_i += sum_k tau_(g^i)(w)[k] bold_t[i][k]
+//                          (and the bar chain with tau_(2n - g^i) and w)          full_packing_offline_mode (:2301-2359)
+//   bold_t_hat = NTT(G^-1(rbar_0)),  a_hat = r_0 + sum_k v[k] bold_t_hat[k] in coefficient form
+// with G^-1 the base-2^b digits (b = floor(32 / tg) + 1, gadget_invert_transposed_alloc, :1468-1493).
+//
+// Two identities let the device skip work the reference does literally:
+//   * perm (util.rs negacyclic_perm, shift 0) is the automorphism X -> X^-1, whose slot table is s -> n - 1 - s;
+//     NTT(hint column) is the hint's accumulator before its inverse transform, so act[j][s] = acc_j[n - 1 - s];
+//   * the packing-matrix fold (sw_pack_build) writes every (column z, slot s, digit k) once: the automorphism that
+//     carries z to s is e = (2 brv(s) + 1) (2 brv(z) + 1)^-1 mod 2n, e = g^i or 2n - g^i, so each byte of the
+//     matrix is a gather from bold_t or bold_t_bar instead of a scatter-add.
+#pragma once
+#include <cstdint>
+#include "hint.cuh"
+#include "modq.cuh"
+
+namespace alto {
+
+constexpr int kActCols = 8;  // database columns per CTA of the act kernel: 8 u32 = one 32-byte sector per slot
+
+__device__ __forceinline__ int brv_bits(int x, int logn) { return (int)(__brev((unsigned)x) >> (32 - logn)); }
+
+// table_t[s] of the automorphism tau_t (t odd, < 2n)
+__device__ __forceinline__ int auto_slot(int t, int s, int n, int logn) {
+  const int e = (t * (2 * brv_bits(s, logn) + 1)) & (2 * n - 1);
+  return brv_bits((e - 1) >> 1, logn);
+}
+
+// g^i mod 2n, or 2n - g^i for the bar chain (g = 5)
+__device__ __forceinline__ int gen_pow(int i, int bar, int n) {
+  int r = 1, b = 5;
+  for (int k = i; k; k >>= 1) {
+    if (k & 1) r = (r * b) & (2 * n - 1);
+    b = (b * b) & (2 * n - 1);
+  }
+  return bar ? 2 * n - r : r;
+}
+
+// Forward transforms of `cnt` polynomials stored back to back in shared memory.
+__device__ __forceinline__ void ntt_fwd_multi(uint32_t *a, int n, int cnt, const uint32_t *__restrict__ psi) {
+  const int half = n >> 1;
+  for (int m = 1, t = half; m < n; m <<= 1, t >>= 1) {
+    for (int b = threadIdx.x; b < cnt * half; b += blockDim.x) {
+      const int p = b / half, bb = b - p * half;
+      const int i = bb / t, j = p * n + 2 * i * t + (bb - i * t);
+      const uint32_t u = a[j], v = mul_q(a[j + t], __ldg(psi + m + i));
+      a[j] = add_q(u, v);
+      a[j + t] = sub_q(u, v);
+    }
+    __syncthreads();
+  }
+}
+
+// acc = INTT(acc) (times n^-1), then its tg base-2^bits digits into dig[k n + s], all in shared memory.
+__device__ __forceinline__ void digits_of(uint32_t *acc, uint32_t *dig, int n, int tg, int bits,
+                                         const uint32_t *__restrict__ psi_inv, uint32_t n_inv) {
+  hint_ntt_inv(acc, n, psi_inv);
+  const uint32_t mask = bits >= 32 ? 0xffffffffu : (1u << bits) - 1u;
+  for (int s = threadIdx.x; s < n; s += blockDim.x) {
+    const uint32_t x = mul_q(acc[s], n_inv);
+    for (int k = 0; k < tg; ++k) dig[k * n + s] = bits * k >= 32 ? 0u : (x >> (bits * k)) & mask;
+  }
+  __syncthreads();
+}
+
+// act, one CTA per kActCols consecutive database columns: acc_c = sum_p NTT(D_(p,c)) . qhat_p (qhat = NTT(perm(q_p))),
+// stored as actT[o][s][j] = acc_c[n - 1 - s] for column c = o n + j.  Database columns come from the engine's tile
+// layout as in hint_ring_kernel.
+__global__ void __launch_bounds__(256) offline_act_kernel(const uint8_t *__restrict__ db, size_t kbs, int n,
+                                                          int polys, const uint32_t *__restrict__ qhat,
+                                                          const uint32_t *__restrict__ psi, uint32_t *__restrict__ act) {
+  extern __shared__ uint32_t osm[];
+  uint32_t *a = osm, *acc = osm + n;
+  const size_t col0 = (size_t)blockIdx.x * kActCols;
+  for (int i = threadIdx.x; i < kActCols * n; i += blockDim.x) acc[i] = 0;
+  for (int c = 0; c < kActCols; ++c) {
+    const size_t col = col0 + c;
+    const uint8_t *row = db + (col / 128) * kbs * 16384 + (col % 128) * 128;
+    for (int p = 0; p < polys; ++p) {
+      __syncthreads();
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const size_t rec = (size_t)p * n + i;
+        a[i] = row[(rec >> 7) * 16384 + (rec & 127)];
+      }
+      __syncthreads();
+      hint_ntt_fwd(a, n, psi);
+      const uint32_t *qh = qhat + (size_t)p * n;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) acc[c * n + i] = add_q(acc[c * n + i], mul_q(a[i], __ldg(qh + i)));
+    }
+  }
+  __syncthreads();
+  const size_t o = col0 / n, j0 = col0 % n;  // kActCols divides n: the CTA's columns share their output
+  for (int idx = threadIdx.x; idx < n * kActCols; idx += blockDim.x) {
+    const int s = idx / kActCols, c = idx - s * kActCols;
+    act[(o * n + s) * n + j0 + c] = acc[c * n + (n - 1 - s)];
+  }
+}
+
+// ev: forward transform of every row of act in place (one CTA per row of n).
+__global__ void __launch_bounds__(256) offline_rows_kernel(uint32_t *__restrict__ rows, int n,
+                                                           const uint32_t *__restrict__ psi) {
+  extern __shared__ uint32_t osm[];
+  uint32_t *r = rows + (size_t)blockIdx.x * n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) osm[i] = r[i];
+  __syncthreads();
+  hint_ntt_fwd(osm, n, psi);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) r[i] = osm[i];
+}
+
+// The backward walk, one CTA per (output o, chain bar): bar 0 walks r with tau_(g^i)(w), bar 1 walks rbar with
+// tau_(2n - g^i)(w).  bt[((o 2 + bar) (n/2 - 1) + i) tg + k][s] = bold_t (bar 0) or bold_t_bar (bar 1); the chain's
+// final r_0 (rbar_0) goes to last[(o 2 + bar) n + s].
+__global__ void __launch_bounds__(1024) offline_walk_kernel(const uint32_t *__restrict__ ev, int n, int logn, int tg,
+                                                            int bits, const uint32_t *__restrict__ w,
+                                                            const uint32_t *__restrict__ psi,
+                                                            const uint32_t *__restrict__ psi_inv, uint32_t n_inv,
+                                                            uint32_t *__restrict__ bt, uint32_t *__restrict__ last) {
+  extern __shared__ uint32_t osm[];
+  uint32_t *cur = osm, *dig = osm + n;
+  const int o = blockIdx.x >> 1, bar = blockIdx.x & 1, half = n >> 1;
+  const uint32_t *evo = ev + (size_t)o * n * n;
+  int e = gen_pow(half - 1, bar, n);
+  for (int s = threadIdx.x; s < n; s += blockDim.x) cur[s] = mul_q(evo[(size_t)auto_slot(e, s, n, logn) * n + s], n_inv);
+  __syncthreads();
+  for (int i = half - 2; i >= 0; --i) {
+    digits_of(cur, dig, n, tg, bits, psi_inv, n_inv);
+    ntt_fwd_multi(dig, n, tg, psi);
+    e = gen_pow(i, bar, n);
+    uint32_t *out = bt + (((size_t)(o * 2 + bar) * (half - 1) + i) * tg) * n;
+    for (int s = threadIdx.x; s < n; s += blockDim.x) {
+      const int ts = auto_slot(e, s, n, logn);
+      uint32_t acc = mul_q(evo[(size_t)ts * n + s], n_inv);
+      for (int k = 0; k < tg; ++k) {
+        const uint32_t d = dig[k * n + s];
+        out[k * n + s] = d;
+        acc = add_q(acc, mul_q(__ldg(w + k * n + ts), d));
+      }
+      cur[s] = acc;
+    }
+    __syncthreads();
+  }
+  for (int s = threadIdx.x; s < n; s += blockDim.x) last[(size_t)(o * 2 + bar) * n + s] = cur[s];
+}
+
+// Per output (one CTA each): bold_t_hat = NTT(G^-1(rbar_0)); a_hat = INTT(r_0 + sum_k v[k] bold_t_hat[k]).  Writes
+// the engine's bold_t_hat (times the tail's scale 2^-log2 n), the row-0 prefix (a_hat rescaled to 2^q2_bits, packed
+// LSB first, the rest of the part zero: switch_prefix_row0, src/modulus_switch.rs:136-147) and, for callers that
+// ask, the plain bold_t_hat and a_hat.
+__global__ void __launch_bounds__(1024) offline_finish_kernel(const uint32_t *__restrict__ last, int n, int tg,
+                                                              int bits, const uint32_t *__restrict__ v,
+                                                              const uint32_t *__restrict__ psi,
+                                                              const uint32_t *__restrict__ psi_inv, uint32_t n_inv,
+                                                              uint32_t tail_scale, uint32_t *__restrict__ that_eng,
+                                                              uint8_t *__restrict__ prefix, size_t part_len,
+                                                              int q2_bits, uint32_t *__restrict__ that_out,
+                                                              uint32_t *__restrict__ a_hat_out) {
+  extern __shared__ uint32_t osm[];
+  uint32_t *cur = osm, *dig = osm + n;
+  const int o = blockIdx.x;
+  const size_t count = (size_t)tg * n;
+  for (int s = threadIdx.x; s < n; s += blockDim.x) cur[s] = last[(size_t)(o * 2 + 1) * n + s];
+  __syncthreads();
+  digits_of(cur, dig, n, tg, bits, psi_inv, n_inv);
+  ntt_fwd_multi(dig, n, tg, psi);
+  for (int s = threadIdx.x; s < n; s += blockDim.x) {
+    uint32_t acc = last[(size_t)(o * 2) * n + s];
+    for (int k = 0; k < tg; ++k) {
+      const uint32_t t = dig[k * n + s];
+      acc = add_q(acc, mul_q(__ldg(v + k * n + s), t));
+      that_eng[o * count + k * n + s] = mul_q(t, tail_scale);
+      if (that_out) that_out[o * count + k * n + s] = t;
+    }
+    cur[s] = acc;
+  }
+  __syncthreads();
+  hint_ntt_inv(cur, n, psi_inv);
+  for (int s = threadIdx.x; s < n; s += blockDim.x) {
+    cur[s] = mul_q(cur[s], n_inv);
+    if (a_hat_out) a_hat_out[(size_t)o * n + s] = cur[s];
+  }
+  __syncthreads();
+  // rescale(a, Q, 2^q2_bits): centre, round half away from zero, reduce (src/modulus_switch.rs:116-130)
+  const int64_t q = kQ32, half = kQ32 / 2, q2 = int64_t(1) << q2_bits;
+  uint8_t *pre = prefix + (size_t)o * part_len;
+  const size_t row0_bytes = ((size_t)q2_bits * n + 7) / 8;
+  for (size_t b = row0_bytes + threadIdx.x; b < part_len; b += blockDim.x) pre[b] = 0;
+  // 8 values of q2_bits bits fill q2_bits whole bytes: thread g packs values 8 g .. 8 g + 7
+  for (int g = threadIdx.x; g < n / 8; g += blockDim.x) {
+    uint8_t bytes[64] = {};
+    for (int u = 0; u < 8; ++u) {
+      const int64_t a = cur[8 * g + u];
+      const int64_t c = a >= half ? a - q : a;
+      int64_t t = (c * q2 + (c >= 0 ? half : -half)) / q;
+      t = ((t % q2) + q2) % q2;
+      for (int bit = 0; bit < q2_bits; ++bit)
+        if ((t >> bit) & 1) bytes[(u * q2_bits + bit) >> 3] |= (uint8_t)(1u << ((u * q2_bits + bit) & 7));
+    }
+    for (int k = 0; k < q2_bits; ++k) pre[(size_t)g * q2_bits + k] = bytes[k];
+  }
+}
+
+// The packing matrix in the engine's tile layout, one thread per value (engine column col, key word kk):
+// U[col][kk] = bold_t[o][i][k][z] (or bold_t_bar) for the automorphism carrying z to s (see the file comment), zero
+// for the two slots no automorphism of the walk reaches; times tail_scale; its 4 bytes go to planes col 4 + j,
+// tile (row / 128, kk / 128) at (mt kbs + kb) 16 KB, byte (row % 128) 128 + kk % 128.
+__global__ void __launch_bounds__(256) offline_planes_kernel(const uint32_t *__restrict__ bt, int n, int logn, int tg,
+                                                             size_t cols, const int16_t *__restrict__ dlog,
+                                                             const uint16_t *__restrict__ inv_odd,
+                                                             uint32_t tail_scale, uint8_t *__restrict__ ub,
+                                                             size_t kbs) {
+  const size_t K = (size_t)tg * n;
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= cols * K) return;
+  const size_t col = idx / K, kk = idx - col * K;
+  const int o = (int)(col / n), z = (int)(col % n), k = (int)(kk / n), s = (int)(kk % n), half = n >> 1;
+  const int t = ((2 * brv_bits(s, logn) + 1) * (int)__ldg(inv_odd + brv_bits(z, logn))) & (2 * n - 1);
+  const int d = __ldg(dlog + ((t - 1) >> 1));
+  uint32_t v = 0;
+  if (d >= 0 && (d >> 1) <= half - 2)
+    v = mul_q(__ldg(bt + (((size_t)(o * 2 + (d & 1)) * (half - 1) + (d >> 1)) * tg + k) * n + z), tail_scale);
+  for (int j = 0; j < 4; ++j) {
+    const size_t row = col * 4 + j;
+    ub[((row >> 7) * kbs + (kk >> 7)) * 16384 + (row & 127) * 128 + (kk & 127)] = (uint8_t)(v >> (8 * j));
+  }
+}
+
+}  // namespace alto

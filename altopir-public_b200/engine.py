@@ -123,6 +123,33 @@ class Engine:
             raise EngineError(f"engine error {r}: {last_error()}")
         return out
 
+    def offline(self, query, w_mask, v_mask, want=False):
+        """alto_engine_offline: the scheme's offline set-up on the device (Prepared::new, src/service.rs:127-157) --
+        hint, InspiRING precomputation, packing matrix, bold_t_hat, row-0 prefixes -- written into this engine.
+        query: (rows / n, n) row-0 query polynomials (-a_i mod Q); w_mask, v_mask: (tg, n) NTT-form masks.
+        Returns the device time in ms, and with want=True also a dict of the per-output bold_t, bold_t_bar, that
+        (bold_t_hat) and a_hat as uint32 arrays."""
+        q = np.ascontiguousarray(query, dtype=np.uint64)
+        w = np.ascontiguousarray(w_mask, dtype=np.uint64)
+        v = np.ascontiguousarray(v_mask, dtype=np.uint64)
+        n = q.shape[1]
+        assert q.size == self.rows and w.size == v.size and w.size % n == 0
+        tg, outputs = w.size // n, self.cols // n
+        out = {}
+        if want:
+            per = (n // 2 - 1) * tg * n
+            out = {"bold_t": np.empty((outputs, per), dtype=np.uint32),
+                   "bold_t_bar": np.empty((outputs, per), dtype=np.uint32),
+                   "that": np.empty((outputs, tg * n), dtype=np.uint32),
+                   "a_hat": np.empty((outputs, n), dtype=np.uint32)}
+        ms = ctypes.c_double(0.0)
+        ptr = (lambda k: _p(out[k]) if want else None)
+        r = lib().alto_engine_offline(self.ptr, _p(q), _p(w), _p(v), ptr("bold_t"), ptr("bold_t_bar"), ptr("that"),
+                                      ptr("a_hat"), ctypes.byref(ms))
+        if r < 0:
+            raise EngineError(f"engine error {r}: {last_error()}")
+        return (ms.value, out) if want else ms.value
+
     def fill_synthetic(self):
         """alto_engine_fill_synthetic: the whole database becomes the synthetic records, generated on the device."""
         r = lib().alto_engine_fill_synthetic(self.ptr)

@@ -291,6 +291,24 @@ void alto_pack_encode(int8_t *ub, const uint32_t *U, size_t cols, size_t K, int 
  * 8 n cols bytes) for the call.  0, -1 for bad arguments or an unsupported n, -4 for a device failure. */
 int alto_hint_ring(void *engine, const uint64_t *query, uint64_t *out, int perm_out);
 
+/* The scheme's offline set-up on the device, for an engine whose database is resident (Prepared::new,
+ * src/service.rs:127-157, over YServer::perform_offline_precomputation_simplepir, src/server.rs:947-1021): the
+ * hint's ring multiply (as alto_hint_ring, kept in NTT form), the InspiRING precomputation of every output
+ * (full_packing_with_preprocessing_offline, src/packing.rs:2260-2359), the packing matrix (sw_pack_build), bold_t_hat
+ * and the row-0 prefixes (switch_prefix_row0), written into the engine in place of the state it was created with,
+ * and the engine's inverse-NTT table set to the ring's.  After it the engine answers requests whose responses
+ * decrypt under the client's secret.
+ *   query: (records / n) x n raw polynomials, row 0 of the query's RLWE ciphertexts (-a_i mod q), as alto_hint_ring;
+ *   w_mask, v_mask: tg x n NTT-form masks of the rotation and conjugation keys (OfflinePackingKeys::init_full).
+ * Ring: Z_q[X]/(X^n + 1), NTT slot s = evaluation at psi^(2 brv(s) + 1), psi the smallest primitive 2n-th root of
+ * unity; gadget digits of floor(32 / tg) + 1 bits.  Optional host outputs (NULL to skip), all u32 in [0, q):
+ * bold_t and bold_t_bar, outputs x (n/2 - 1) x tg x n each; that (bold_t_hat), outputs x tg x n; a_hat, outputs x n.
+ * ms (optional) receives the device time of the set-up.  Waits for the engine's batches in flight; allocates about
+ * 4 n cols + 8 cols tg n bytes of device scratch for the call.  0, -1 for bad arguments or an unsupported
+ * configuration, -4 for a device failure. */
+int alto_engine_offline(void *engine, const uint64_t *query, const uint64_t *w_mask, const uint64_t *v_mask,
+                        uint32_t *bold_t, uint32_t *bold_t_bar, uint32_t *that, uint32_t *a_hat, double *ms);
+
 /* Self-check of the engine's modulus-switch arithmetic on the host: sum over v in [v0, v1) of rescale(v) * (2v + 1)
  * modulo 2^64, where rescale is the exact integer centred rescale Q -> q1 that the tail kernel runs. */
 uint64_t alto_rescale_digest(uint64_t q1, uint64_t v0, uint64_t v1, int threads);

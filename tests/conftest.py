@@ -58,3 +58,18 @@ def gpu():
 def sha(a):
     import hashlib
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+@pytest.fixture(scope="session")
+def client_mod():
+    from altopir_b200 import client
+    return client
+
+
+@pytest.fixture(scope="session")
+def scheme_state(oracle, svc):
+    """Engine state of the scheme itself (hint, InspiRING precomputation, prefixes) for a 4 MiB database of 2048
+    synthetic records x 2048 bytes, built by the oracle's numpy restatement: requests of the client decrypt over it."""
+    from oracle.scheme import SchemeState
+    p = svc.params(2048, 2048)
+    return SchemeState(p, oracle.synthetic_db_col(p.rows, 0, p.record_bytes), oracle)

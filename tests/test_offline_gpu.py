@@ -1,0 +1,82 @@
+"""The scheme's offline set-up on the device (alto_engine_offline: hint, InspiRING precomputation, packing matrix,
+bold_t_hat, prefixes) against the oracle's numpy restatement, and decryption round trips through this engine:
+requests of the client restatement, answered on the GPU, decrypt to the records asked for (the check
+tests/engine.rs makes of the reference)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _clients(client_mod, p, idx, seed0):
+    clients = [client_mod.Client(p, seed=seed0 + k) for k in range(len(idx))]
+    return clients, [c.request(i) for c, i in zip(clients, idx)]
+
+
+def _answer(e, frames):
+    b = len(frames)
+    out = np.zeros((b, e.response_len()), dtype=np.uint8)
+    status = np.full(b, -1, dtype=np.int32)
+    r, _ = e.answer(frames, out, status)
+    assert r == b and list(status) == [0] * b
+    return out
+
+
+def test_engine_over_the_oracle_scheme_state_decrypts(gpu, eng, client_mod, oracle, scheme_state):
+    """The engine alone, given the oracle's scheme state (packing matrix from this library's sw_pack_build)."""
+    st, p = scheme_state, scheme_state.p
+    ub = np.empty(4 * p.record_bytes * p.count, dtype=np.int8)
+    eng.build_packing_matrix(ub, st.bold_t, st.bold_t_bar, st.tables, st.gen_pows, p.n // 2 - 1, p.tg, p.n)
+    tiled = eng.TiledDb(st.db_col, st.db_col.shape[1], p.rows, p.record_bytes)
+    e = eng.Engine(st.db_col, tiled, st.db_col.shape[1], ub, p.n, p.tg, st.prefixes, p.row1_off, 1 << p.q1_bits,
+                   p.q1_bits, st.that, st.inv_table)
+    try:
+        idx = [3, 999, p.rows - 1]
+        clients, frames = _clients(client_mod, p, idx, 40)
+        out = _answer(e, frames)
+        _, _, want = oracle.answer(st, frames)
+        assert np.array_equal(out, want)
+        for c, resp, i in zip(clients, out, idx):
+            assert np.array_equal(c.decrypt(resp), oracle.synthetic_record(i, p.record_bytes))
+    finally:
+        e.close()
+
+
+def test_device_offline_matches_the_oracle_restatement(gpu, client_mod, oracle, scheme_state):
+    from altopir_b200 import offline
+    st, p = scheme_state, scheme_state.p
+    e = offline.blank_engine(p, st.db_col)
+    try:
+        ms, out = offline.prepare(e, p, want=True)
+        assert ms > 0
+        assert np.array_equal(out["bold_t"][0].astype(np.uint64), st.bold_t[0])
+        assert np.array_equal(out["bold_t_bar"][0].astype(np.uint64), st.bold_t_bar[0])
+        assert np.array_equal(out["that"][0].astype(np.uint64), st.that[0])
+        assert np.array_equal(out["a_hat"][0].astype(np.uint64), st.a_hat[0])
+        idx = [0, 1500, 2047]
+        clients, frames = _clients(client_mod, p, idx, 50)
+        got = _answer(e, frames)
+        _, _, want = oracle.answer(st, frames)
+        assert np.array_equal(got, want)          # packing matrix, bold_t_hat, prefixes and table as the oracle's
+        for c, resp, i in zip(clients, got, idx):
+            assert np.array_equal(c.decrypt(resp), oracle.synthetic_record(i, p.record_bytes))
+    finally:
+        e.close()
+
+
+@pytest.mark.parametrize("rows,record_bytes", [(32768, 4096), (32768, 32768)])
+def test_device_offline_round_trip(gpu, client_mod, svc, rows, record_bytes):
+    """A database of synthetic records generated on the device, its scheme state built on the device, answered in
+    one batch: every response decrypts to its record (1 GiB at the second size)."""
+    from altopir_b200 import offline
+    p = svc.params(rows, record_bytes)
+    e, ms = offline.scheme_engine(p)
+    try:
+        idx = [0, 12345, rows // 2 + 7, rows - 1]
+        clients, frames = _clients(client_mod, p, idx, 60)
+        out = _answer(e, frames)
+        for c, resp, i in zip(clients, out, idx):
+            assert np.array_equal(c.decrypt(resp), svc.synthetic_record(i, record_bytes))
+        print(f"offline set-up of {rows} x {record_bytes} B on the device: {ms:.1f} ms")
+    finally:
+        e.close()
