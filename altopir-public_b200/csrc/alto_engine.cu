@@ -1917,6 +1917,14 @@ int alto_engine_offline(void *p, const uint64_t *query, const uint64_t *w_mask, 
   step(cudaFuncSetAttribute(alto::offline_act_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)act_smem));
   step(cudaFuncSetAttribute(alto::offline_walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)walk_smem));
   step(cudaFuncSetAttribute(alto::offline_finish_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)walk_smem));
+  // the walk's cluster: one CTA per gadget digit, at most 8 (the portable cluster size); ALTO_OFFLINE_CLUSTER=1 runs
+  // the single-CTA walk
+  int cluster = (int)std::min<size_t>(tg, 8);
+  if (const char *v = getenv("ALTO_OFFLINE_CLUSTER")) cluster = std::max(1, std::min(8, atoi(v)));
+  const size_t cwalk_smem = (2 + (tg + cluster - 1) / cluster) * n * sizeof(uint32_t);
+  if (cluster > 1)
+    step(cudaFuncSetAttribute(alto::offline_walk_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)cwalk_smem));
   const unsigned nt = (unsigned)std::max<size_t>(32, std::min<size_t>(256, n / 2));
   const unsigned wt = (unsigned)std::max<size_t>(64, std::min<size_t>(1024, tg * n / 2));
   const uint32_t tail_scale = alto::inv_pow2_q(logn);
@@ -1931,8 +1939,27 @@ int alto_engine_offline(void *p, const uint64_t *query, const uint64_t *w_mask, 
     step(cudaGetLastError());
     alto::offline_rows_kernel<<<(unsigned)cols, nt, n * sizeof(uint32_t)>>>(d_act, (int)n, d_psi);
     step(cudaGetLastError());
-    alto::offline_walk_kernel<<<(unsigned)(outputs * 2), wt, walk_smem>>>(d_act, (int)n, logn, (int)tg, bits, d_w,
-                                                                          d_psi, d_psi_inv, n_inv, d_bt, d_last);
+    if (cluster > 1) {
+      // one cluster of `cluster` CTAs per (output, chain), the digits split between them
+      cudaLaunchConfig_t cfg = {};
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = (unsigned)cluster;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.gridDim = dim3((unsigned)(outputs * 2 * cluster));
+      cfg.blockDim = dim3(wt);
+      cfg.dynamicSmemBytes = cwalk_smem;
+      cfg.stream = 0;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      step(cudaLaunchKernelEx(&cfg, alto::offline_walk_cluster_kernel, (const uint32_t *)d_act, (int)n, logn,
+                              (int)tg, bits, (const uint32_t *)d_w, (const uint32_t *)d_psi,
+                              (const uint32_t *)d_psi_inv, n_inv, d_bt, d_last));
+    } else {
+      alto::offline_walk_kernel<<<(unsigned)(outputs * 2), wt, walk_smem>>>(d_act, (int)n, logn, (int)tg, bits, d_w,
+                                                                            d_psi, d_psi_inv, n_inv, d_bt, d_last);
+    }
     step(cudaGetLastError());
     alto::offline_finish_kernel<<<(unsigned)outputs, wt, walk_smem>>>(d_last, (int)n, (int)tg, bits, d_v, d_psi,
                                                                       d_psi_inv, n_inv, tail_scale, e->d_that,

@@ -23,6 +23,7 @@
 //     carries z to s is e = (2 brv(s) + 1) (2 brv(z) + 1)^-1 mod 2n, e = g^i or 2n - g^i, so each byte of the
 //     matrix is a gather from bold_t or bold_t_bar instead of a scatter-add.
 #pragma once
+#include <cooperative_groups.h>
 #include <cstdint>
 #include "hint.cuh"
 #include "modq.cuh"
@@ -153,6 +154,66 @@ __global__ void __launch_bounds__(1024) offline_walk_kernel(const uint32_t *__re
     __syncthreads();
   }
   for (int s = threadIdx.x; s < n; s += blockDim.x) last[(size_t)(o * 2 + bar) * n + s] = cur[s];
+}
+
+// The same walk with one thread-block cluster of C CTAs per (output, chain): every CTA runs the step's inverse
+// transform (the same values in each), takes the digits k = c, c + C, ... of its rank c, transforms them and forms
+// its part of sum_k tau(w)[k] bold_t[i][k]; the parts are summed through distributed shared memory.  A step costs
+// two transforms instead of 1 + tg.  Launched with cluster dimensions (C, 1, 1): CTAs C q .. C q + C - 1 are chain q.
+__global__ void __launch_bounds__(1024) offline_walk_cluster_kernel(const uint32_t *__restrict__ ev, int n, int logn,
+                                                                    int tg, int bits, const uint32_t *__restrict__ w,
+                                                                    const uint32_t *__restrict__ psi,
+                                                                    const uint32_t *__restrict__ psi_inv,
+                                                                    uint32_t n_inv, uint32_t *__restrict__ bt,
+                                                                    uint32_t *__restrict__ last) {
+  namespace cg = cooperative_groups;
+  extern __shared__ uint32_t osm[];
+  cg::cluster_group cl = cg::this_cluster();
+  const int C = (int)cl.num_blocks(), c = (int)cl.block_rank();
+  const int chain = blockIdx.x / C, o = chain >> 1, bar = chain & 1, half = n >> 1;
+  const int kper = (tg + C - 1) / C;
+  uint32_t *cur = osm, *part = osm + n, *dig = osm + 2 * n;
+  const uint32_t mask = bits >= 32 ? 0xffffffffu : (1u << bits) - 1u;
+  const uint32_t *evo = ev + (size_t)o * n * n;
+  int e = gen_pow(half - 1, bar, n);
+  for (int s = threadIdx.x; s < n; s += blockDim.x) cur[s] = mul_q(evo[(size_t)auto_slot(e, s, n, logn) * n + s], n_inv);
+  __syncthreads();
+  for (int i = half - 2; i >= 0; --i) {
+    hint_ntt_inv(cur, n, psi_inv);
+    for (int s = threadIdx.x; s < n; s += blockDim.x) {
+      const uint32_t x = mul_q(cur[s], n_inv);
+      for (int j = 0; j < kper; ++j) {
+        const int k = c + C * j;
+        dig[j * n + s] = (k < tg && bits * k < 32) ? (x >> (bits * k)) & mask : 0u;
+      }
+    }
+    __syncthreads();
+    ntt_fwd_multi(dig, n, kper, psi);
+    e = gen_pow(i, bar, n);
+    uint32_t *out = bt + (((size_t)chain * (half - 1) + i) * tg) * n;
+    for (int s = threadIdx.x; s < n; s += blockDim.x) {
+      const int ts = auto_slot(e, s, n, logn);
+      uint32_t p = 0;
+      for (int j = 0; j < kper; ++j) {
+        const int k = c + C * j;
+        if (k < tg) {
+          const uint32_t d = dig[j * n + s];
+          out[k * n + s] = d;
+          p = add_q(p, mul_q(__ldg(w + k * n + ts), d));
+        }
+      }
+      part[s] = p;
+    }
+    cl.sync();  // every CTA's part is written
+    for (int s = threadIdx.x; s < n; s += blockDim.x) {
+      uint32_t acc = mul_q(evo[(size_t)auto_slot(e, s, n, logn) * n + s], n_inv);
+      for (int r = 0; r < C; ++r) acc = add_q(acc, cl.map_shared_rank(part, r)[s]);
+      cur[s] = acc;
+    }
+    cl.sync();  // every CTA has read the parts (they are rewritten next step) and holds the whole new r_i
+  }
+  if (c == 0)
+    for (int s = threadIdx.x; s < n; s += blockDim.x) last[(size_t)chain * n + s] = cur[s];
 }
 
 // Per output (one CTA each): bold_t_hat = NTT(G^-1(rbar_0)); a_hat = INTT(r_0 + sum_k v[k] bold_t_hat[k]).  Writes

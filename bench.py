@@ -590,13 +590,15 @@ def engine_for(svc, eng, p, host_db):
     return st, e
 
 
-def measure_offline(svc, a, reps=3):
-    """The scheme's offline set-up on the device at the workload's shape (alto_engine_offline over the synthetic
-    records generated in HBM: hint, InspiRING precomputation, packing matrix, bold_t_hat, prefixes), device time of
-    `reps` runs, then requests of the client restatement answered by the engine and decrypted."""
+def measure_offline(svc, p, e=None, reps=3):
+    """The scheme's offline set-up on the device (alto_engine_offline: hint, InspiRING precomputation, packing matrix,
+    bold_t_hat, row-0 prefixes, built in HBM for the resident synthetic records), device time of `reps` runs, then
+    requests of the client restatement answered by the engine and decrypted.  `e`: an engine over the synthetic
+    records whose state may be replaced (a fresh one is made and closed otherwise)."""
     from altopir_b200 import client, offline
-    p = svc.params(a.rows, a.record_bytes)
-    e = offline.blank_engine(p)
+    own = e is None
+    if own:
+        e = offline.blank_engine(p)
     try:
         ms = sorted(offline.prepare(e, p) for _ in range(reps))
         idx = [0, p.rows // 3, p.rows - 1]
@@ -608,12 +610,16 @@ def measure_offline(svc, a, reps=3):
         ok = all(np.array_equal(c.decrypt(out[k]), svc.synthetic_record(i, p.record_bytes))
                  for k, (c, i) in enumerate(zip(clients, idx)))
     finally:
-        e.close()
-    return {"what": "alto_engine_offline: the scheme's hint, InspiRING precomputation, packing matrix, bold_t_hat and "
-                    "row-0 prefixes built in HBM for the resident database (Prepared::new)",
-            "config": f"{p.rows} records x {p.record_bytes} B", "device_ms_min": ms[0],
-            "device_ms_median": ms[len(ms) // 2], "runs": reps,
-            "decrypts": bool(ok), "requests_decrypted": len(idx)}
+        if own:
+            e.close()
+    return {"config": f"{p.rows} records x {p.record_bytes} B", "device_ms_min": ms[0],
+            "device_ms_median": ms[len(ms) // 2], "runs": reps, "decrypts": bool(ok),
+            "requests_decrypted": len(idx)}
+
+
+OFFLINE_WHAT = ("alto_engine_offline: the scheme's hint, InspiRING precomputation, packing matrix, bold_t_hat and "
+                "row-0 prefixes built in HBM for the resident database (Prepared::new); then requests of the client "
+                "restatement answered and decrypted")
 
 
 def main_ours(a):
@@ -693,6 +699,7 @@ def main_ours(a):
 
     # ---- the larger databases (rank 0 of a one-GPU run): blocks of up to K steps, about 0.2 s each
     configs = []
+    want_offline, offline_runs = rank == 0 and world == 1 and not a.no_offline, []
     if world == 1 and not a.no_configs:
         for rows, batches, plain_q in SUB_CONFIGS:
             pp = svc.params(rows, a.record_bytes)
@@ -716,10 +723,14 @@ def main_ours(a):
                 print(f"config {rows} records, B = {B}: {r['value']:.0f} QPS device, {r['e2e']['value']:.0f} e2e, "
                       f"frac {r['roofline']['frac']:.3f}", file=sys.stderr, flush=True)
                 m.close()
+            if want_offline:
+                offline_runs.append(measure_offline(svc, pp, e))
             e.close()
             torch.cuda.empty_cache()
     sampler.stop()
-    offline_setup = measure_offline(svc, a) if rank == 0 and world == 1 and not a.no_offline else None
+    if want_offline:
+        offline_runs.insert(0, measure_offline(svc, p))
+    offline_setup = {"what": OFFLINE_WHAT, "runs": offline_runs} if want_offline else None
 
     if rank == 0:
         pub = PUBLISHED_QPS.get(a.rows) if (a.batch == 128 and a.record_bytes == 32768) else None
