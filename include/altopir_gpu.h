@@ -303,8 +303,9 @@ int alto_hint_ring(void *engine, const uint64_t *query, uint64_t *out, int perm_
  * Ring: Z_q[X]/(X^n + 1), NTT slot s = evaluation at psi^(2 brv(s) + 1), psi the smallest primitive 2n-th root of
  * unity; gadget digits of floor(32 / tg) + 1 bits.  Optional host outputs (NULL to skip), all u32 in [0, q):
  * bold_t and bold_t_bar, outputs x (n/2 - 1) x tg x n each; that (bold_t_hat), outputs x tg x n; a_hat, outputs x n.
- * ms (optional) receives the device time of the set-up.  Waits for the engine's batches in flight; allocates about
- * 4 n cols + 8 cols tg n bytes of device scratch for the call.  0, -1 for bad arguments or an unsupported
+ * ms (optional) receives the device time of the set-up.  Waits for the engine's batches in flight (a serving loop
+ * must not run on the engine meanwhile); allocates about 4 n cols + 4 tg n cols + 12 records bytes of device scratch
+ * for the call (1.3 GB at 32 KB records, n = 2048, tg = 4).  0, -1 for bad arguments or an unsupported
  * configuration, -4 for a device failure. */
 int alto_engine_offline(void *engine, const uint64_t *query, const uint64_t *w_mask, const uint64_t *v_mask,
                         uint32_t *bold_t, uint32_t *bold_t_bar, uint32_t *that, uint32_t *a_hat, double *ms);

@@ -129,3 +129,13 @@ def test_query_rejects_an_index_out_of_range(client_mod, svc):
     p = svc.params(2048, 2048)
     with pytest.raises(ValueError):
         client_mod.Client(p, seed=1).query(p.rows)
+
+
+def test_offline_public_inputs_are_the_client_masks(client_mod, svc):
+    from altopir_b200 import offline
+    p = svc.params(4096, 2048)
+    q, w, v = offline.public_inputs(p)
+    a = client_mod.query_masks(p.rows, p.n)
+    assert q.shape == (p.rows // p.n, p.n) and np.array_equal((q + a) % client_mod.Q, np.zeros_like(a))
+    w2, v2 = client_mod.packing_masks(p.n, p.tg)
+    assert np.array_equal(w, w2) and np.array_equal(v, v2) and not np.array_equal(w, v)

@@ -80,3 +80,22 @@ def test_device_offline_round_trip(gpu, client_mod, svc, rows, record_bytes):
         print(f"offline set-up of {rows} x {record_bytes} B on the device: {ms:.1f} ms")
     finally:
         e.close()
+
+
+def test_device_offline_rejects_bad_arguments(gpu, svc):
+    import ctypes
+    from altopir_b200 import lib, offline
+    p = svc.params(2048, 2048)
+    e = offline.blank_engine(p, np.zeros((p.record_bytes, p.rows), dtype=np.uint8))
+    try:
+        q, w, v = offline.public_inputs(p)
+        assert lib().alto_engine_offline(e.ptr, None, w.ctypes.data, v.ctypes.data, None, None, None, None,
+                                         None) == -1
+        assert lib().alto_engine_offline(None, q.ctypes.data, w.ctypes.data, v.ctypes.data, None, None, None, None,
+                                         None) == -1
+        assert "bad arguments" in lib().alto_last_error().decode()
+        ms = ctypes.c_double(-1.0)
+        assert lib().alto_engine_offline(e.ptr, q.ctypes.data, w.ctypes.data, v.ctypes.data, None, None, None, None,
+                                         ctypes.byref(ms)) == 0 and ms.value > 0
+    finally:
+        e.close()
