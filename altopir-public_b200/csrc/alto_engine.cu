@@ -1915,6 +1915,13 @@ int alto_engine_offline(void *p, const uint64_t *query, const uint64_t *w_mask, 
   step(cudaMemcpy(d_inv_odd, inv_odd.data(), n * sizeof(uint16_t), cudaMemcpyHostToDevice));
   const size_t act_smem = (1 + alto::kActCols) * n * sizeof(uint32_t), walk_smem = (1 + tg) * n * sizeof(uint32_t);
   step(cudaFuncSetAttribute(alto::offline_act_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)act_smem));
+  // n = 2048: the act kernel with register transforms (ALTO_OFFLINE_ACT8=0 runs the shared-memory one)
+  bool act8 = true;
+  if (const char *v = getenv("ALTO_OFFLINE_ACT8")) act8 = v[0] != '0';
+  const size_t act8_smem = (2 + alto::kActCols) * n * sizeof(uint32_t);
+  if (n == 2048)
+    step(cudaFuncSetAttribute(alto::offline_act8_kernel<11>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)act8_smem));
   step(cudaFuncSetAttribute(alto::offline_walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)walk_smem));
   step(cudaFuncSetAttribute(alto::offline_finish_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)walk_smem));
   // the walk's cluster: one CTA per gadget digit, at most 8 (the portable cluster size); ALTO_OFFLINE_CLUSTER=1 runs
@@ -1934,8 +1941,13 @@ int alto_engine_offline(void *p, const uint64_t *query, const uint64_t *w_mask, 
     // the hint's query: NTT(perm(q_p)), without the n^-1 the coefficient-domain hint folds in
     alto::hint_query_kernel<<<(unsigned)polys, nt, n * sizeof(uint32_t)>>>(d_q, (int)n, d_psi, 1u, d_qhat);
     step(cudaGetLastError());
-    alto::offline_act_kernel<<<(unsigned)(cols / alto::kActCols), 256, act_smem>>>(e->d_db, e->db_kbs, (int)n,
-                                                                                  (int)polys, d_qhat, d_psi, d_act);
+    if (n == 2048 && act8) {
+      alto::offline_act8_kernel<11><<<(unsigned)(cols / alto::kActCols), 256, act8_smem>>>(
+          e->d_db, e->db_kbs, (int)polys, d_qhat, d_psi, d_act);
+    } else {
+      alto::offline_act_kernel<<<(unsigned)(cols / alto::kActCols), 256, act_smem>>>(e->d_db, e->db_kbs, (int)n,
+                                                                                    (int)polys, d_qhat, d_psi, d_act);
+    }
     step(cudaGetLastError());
     alto::offline_rows_kernel<<<(unsigned)cols, nt, n * sizeof(uint32_t)>>>(d_act, (int)n, d_psi);
     step(cudaGetLastError());

@@ -110,6 +110,111 @@ __global__ void __launch_bounds__(256) offline_act_kernel(const uint8_t *__restr
   }
 }
 
+// Positions of a thread's 8 values in a round of s forward stages that starts at half-size t (n / 8 threads; each
+// holds 8 / 2^s groups of 2^s values): group grp = g + q n/8 is block blk = grp / d, offset r = grp % d, d = 2t / 2^s,
+// and its value b sits at blk 2t + r + b d.
+template <int L>
+__device__ __forceinline__ int fwd_pos(int g, int q, int b, int s, int t) {
+  const int G = 1 << s, d = 2 * t / G, grp = g + q * ((1 << L) / 8);
+  return (grp / d) * 2 * t + grp % d + b * d;
+}
+
+// One round of s Cooley-Tukey stages (Longa-Naehrig Algorithm 1) on the thread's values: stage k of the round has
+// half-size t >> k and m << k blocks; its pairs are b, b + 2^(s-1-k) inside a group, twiddle psi[(m << k) + (blk << k) +
+// (b >> (s - k))].
+template <int L>
+__device__ __forceinline__ void fwd_round(uint32_t (&x)[8], int g, int s, int m, int t,
+                                          const uint32_t *__restrict__ psi) {
+  const int G = 1 << s, d = 2 * t / G;
+#pragma unroll
+  for (int q = 0; q < 8 / G; ++q) {
+    const int blk = (g + q * ((1 << L) / 8)) / d;
+#pragma unroll
+    for (int k = 0; k < s; ++k) {
+      const int half = G >> (k + 1);
+#pragma unroll
+      for (int b = 0; b < G; ++b) {
+        if (b & half) continue;
+        const uint32_t w = __ldg(psi + (m << k) + (blk << k) + (b >> (s - k)));
+        const uint32_t u = x[q * G + b], v = mul_q(x[q * G + b + half], w);
+        x[q * G + b] = add_q(u, v);
+        x[q * G + b + half] = sub_q(u, v);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ int act_swz(int pos) { return pos ^ ((pos >> 5) & 31); }
+
+// The act kernel with the transforms in registers: n / 8 threads, 8 values each, three stages per round and one
+// shared-memory exchange between rounds (double-buffered: one barrier an exchange), against a barrier per stage in
+// offline_act_kernel.  Same output.
+template <int L>
+__global__ void __launch_bounds__((1 << L) / 8) offline_act8_kernel(const uint8_t *__restrict__ db, size_t kbs,
+                                                                     int polys, const uint32_t *__restrict__ qhat,
+                                                                     const uint32_t *__restrict__ psi,
+                                                                     uint32_t *__restrict__ act) {
+  constexpr int n = 1 << L, NT = n / 8;
+  extern __shared__ uint32_t osm[];
+  uint32_t *accs = osm + 2 * n;  // [column in CTA][position]
+  const int g = threadIdx.x;
+  const size_t col0 = (size_t)blockIdx.x * kActCols;
+  int ex = 0;  // exchanges so far: buffer ex & 1
+  for (int c = 0; c < kActCols; ++c) {
+    const size_t col = col0 + c;
+    const uint8_t *row = db + (col / 128) * kbs * 16384 + (col % 128) * 128;
+    uint32_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int p = 0; p < polys; ++p) {
+      uint32_t x[8];
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {  // the first round's positions: g + b n / 8
+        const size_t rec = (size_t)p * n + g + b * NT;
+        x[b] = row[(rec >> 7) * 16384 + (rec & 127)];
+      }
+#pragma unroll
+      for (int s0 = 0; s0 < L; s0 += 3) {
+        const int s = (L - s0) < 3 ? (L - s0) : 3, t = n >> (s0 + 1);
+        if (s0 > 0) {
+          const int ps = 3, pt = n >> (s0 - 3 + 1);  // every round before the last has three stages
+          uint32_t *buf = osm + (ex & 1) * n;
+#pragma unroll
+          for (int q = 0; q < 8 / (1 << ps); ++q)
+#pragma unroll
+            for (int b = 0; b < (1 << ps); ++b) buf[act_swz(fwd_pos<L>(g, q, b, ps, pt))] = x[q * (1 << ps) + b];
+          __syncthreads();
+#pragma unroll
+          for (int q = 0; q < 8 / (1 << s); ++q)
+#pragma unroll
+            for (int b = 0; b < (1 << s); ++b) x[q * (1 << s) + b] = buf[act_swz(fwd_pos<L>(g, q, b, s, t))];
+          ++ex;
+        }
+        fwd_round<L>(x, g, s, 1 << s0, t, psi);
+      }
+      constexpr int ls = (L % 3) ? (L % 3) : 3, lt = n >> (L - ls + 1);  // the last round
+      const uint32_t *qh = qhat + (size_t)p * n;
+#pragma unroll
+      for (int q = 0; q < 8 / (1 << ls); ++q)
+#pragma unroll
+        for (int b = 0; b < (1 << ls); ++b) {
+          const int i = q * (1 << ls) + b;
+          acc[i] = add_q(acc[i], mul_q(x[i], __ldg(qh + fwd_pos<L>(g, q, b, ls, lt))));
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 8 / (1 << ((L % 3) ? (L % 3) : 3)); ++q) {
+      constexpr int ls = (L % 3) ? (L % 3) : 3, lt = n >> (L - ls + 1);
+#pragma unroll
+      for (int b = 0; b < (1 << ls); ++b) accs[c * n + fwd_pos<L>(g, q, b, ls, lt)] = acc[q * (1 << ls) + b];
+    }
+  }
+  __syncthreads();
+  const size_t o = col0 / n, j0 = col0 % n;
+  for (int idx = threadIdx.x; idx < n * kActCols; idx += NT) {
+    const int s = idx / kActCols, c = idx - s * kActCols;
+    act[(o * n + s) * n + j0 + c] = accs[c * n + (n - 1 - s)];
+  }
+}
+
 // ev: forward transform of every row of act in place (one CTA per row of n).
 __global__ void __launch_bounds__(256) offline_rows_kernel(uint32_t *__restrict__ rows, int n,
                                                            const uint32_t *__restrict__ psi) {
