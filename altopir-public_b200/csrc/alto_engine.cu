@@ -1932,8 +1932,16 @@ int alto_engine_offline(void *p, const uint64_t *query, const uint64_t *w_mask, 
   if (cluster > 1)
     step(cudaFuncSetAttribute(alto::offline_walk_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)cwalk_smem));
+  // n = 2048 with one digit a CTA: the walk with register transforms (ALTO_OFFLINE_WALK8=0 runs the other)
+  bool walk8 = n == 2048 && cluster == (int)tg;
+  if (const char *v = getenv("ALTO_OFFLINE_WALK8")) walk8 = walk8 && v[0] != '0';
+  const size_t walk8_smem = (2 + 2 * (size_t)cluster) * n * sizeof(uint32_t);
+  if (walk8)
+    step(cudaFuncSetAttribute(alto::offline_walk8_kernel<11>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)walk8_smem));
   const unsigned nt = (unsigned)std::max<size_t>(32, std::min<size_t>(256, n / 2));
-  const unsigned wt = (unsigned)std::max<size_t>(64, std::min<size_t>(1024, tg * n / 2));
+  // walk and finish threads: at least n / 4 (the cluster walk gathers 4 slots a thread ahead), at most 1024
+  const unsigned wt = (unsigned)std::max<size_t>(std::max<size_t>(64, n / 4), std::min<size_t>(1024, tg * n / 2));
   const uint32_t tail_scale = alto::inv_pow2_q(logn);
   const size_t K = tg * n, planes_threads = cols * K;
   if (err == cudaSuccess) {
@@ -1965,9 +1973,17 @@ int alto_engine_offline(void *p, const uint64_t *query, const uint64_t *w_mask, 
       cfg.stream = 0;
       cfg.attrs = attr;
       cfg.numAttrs = 1;
-      step(cudaLaunchKernelEx(&cfg, alto::offline_walk_cluster_kernel, (const uint32_t *)d_act, (int)n, logn,
-                              (int)tg, bits, (const uint32_t *)d_w, (const uint32_t *)d_psi,
-                              (const uint32_t *)d_psi_inv, n_inv, d_bt, d_last));
+      if (walk8) {  // n = 2048, one digit a CTA: both transforms in registers
+        cfg.blockDim = dim3((unsigned)(n / 8));
+        cfg.dynamicSmemBytes = walk8_smem;
+        step(cudaLaunchKernelEx(&cfg, alto::offline_walk8_kernel<11>, (const uint32_t *)d_act, (int)tg, bits,
+                                (const uint32_t *)d_w, (const uint32_t *)d_psi, (const uint32_t *)d_psi_inv, n_inv,
+                                d_bt, d_last));
+      } else {
+        step(cudaLaunchKernelEx(&cfg, alto::offline_walk_cluster_kernel, (const uint32_t *)d_act, (int)n, logn,
+                                (int)tg, bits, (const uint32_t *)d_w, (const uint32_t *)d_psi,
+                                (const uint32_t *)d_psi_inv, n_inv, d_bt, d_last));
+      }
     } else {
       alto::offline_walk_kernel<<<(unsigned)(outputs * 2), wt, walk_smem>>>(d_act, (int)n, logn, (int)tg, bits, d_w,
                                                                             d_psi, d_psi_inv, n_inv, d_bt, d_last);

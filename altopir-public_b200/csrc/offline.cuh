@@ -26,6 +26,7 @@
 #include <cooperative_groups.h>
 #include <cstdint>
 #include "hint.cuh"
+#include "kernels.cuh"
 #include "modq.cuh"
 
 namespace alto {
@@ -283,7 +284,16 @@ __global__ void __launch_bounds__(1024) offline_walk_cluster_kernel(const uint32
   int e = gen_pow(half - 1, bar, n);
   for (int s = threadIdx.x; s < n; s += blockDim.x) cur[s] = mul_q(evo[(size_t)auto_slot(e, s, n, logn) * n + s], n_inv);
   __syncthreads();
+  constexpr int kAgg = 4;  // slots a thread gathers ahead (n <= kAgg blockDim.x)
   for (int i = half - 2; i >= 0; --i) {
+    // this step's aggregate r_i, loaded before the transforms so that its latency hides behind them
+    e = gen_pow(i, bar, n);
+    uint32_t agg[kAgg];
+#pragma unroll
+    for (int j = 0; j < kAgg; ++j) {
+      const int s = threadIdx.x + j * (int)blockDim.x;
+      agg[j] = s < n ? evo[(size_t)auto_slot(e, s, n, logn) * n + s] : 0u;
+    }
     hint_ntt_inv(cur, n, psi_inv);
     for (int s = threadIdx.x; s < n; s += blockDim.x) {
       const uint32_t x = mul_q(cur[s], n_inv);
@@ -294,7 +304,6 @@ __global__ void __launch_bounds__(1024) offline_walk_cluster_kernel(const uint32
     }
     __syncthreads();
     ntt_fwd_multi(dig, n, kper, psi);
-    e = gen_pow(i, bar, n);
     uint32_t *out = bt + (((size_t)chain * (half - 1) + i) * tg) * n;
     for (int s = threadIdx.x; s < n; s += blockDim.x) {
       const int ts = auto_slot(e, s, n, logn);
@@ -310,8 +319,11 @@ __global__ void __launch_bounds__(1024) offline_walk_cluster_kernel(const uint32
       part[s] = p;
     }
     cl.sync();  // every CTA's part is written
-    for (int s = threadIdx.x; s < n; s += blockDim.x) {
-      uint32_t acc = mul_q(evo[(size_t)auto_slot(e, s, n, logn) * n + s], n_inv);
+#pragma unroll
+    for (int j = 0; j < kAgg; ++j) {
+      const int s = threadIdx.x + j * (int)blockDim.x;
+      if (s >= n) break;
+      uint32_t acc = mul_q(agg[j], n_inv);
       for (int r = 0; r < C; ++r) acc = add_q(acc, cl.map_shared_rank(part, r)[s]);
       cur[s] = acc;
     }
@@ -319,6 +331,123 @@ __global__ void __launch_bounds__(1024) offline_walk_cluster_kernel(const uint32
   }
   if (c == 0)
     for (int s = threadIdx.x; s < n; s += blockDim.x) last[(size_t)chain * n + s] = cur[s];
+}
+
+// The cluster walk with both transforms in registers, for tg CTAs a cluster (one digit each) and n = 2^L: n / 8
+// threads hold 8 values each.  The inverse transform runs the tail kernel's Gentleman-Sande rounds (tail_round: the
+// thread's 8 consecutive slots first, then three stages per shared-memory exchange); the digit goes back through
+// shared memory in natural order and the forward transform runs fwd_round's Cooley-Tukey rounds; the thread then holds
+// slots 8 g .. 8 g + 7 of the next r_i in registers.  Every exchange is double-buffered (one barrier each).
+template <int L>
+__global__ void __launch_bounds__((1 << L) / 8) offline_walk8_kernel(const uint32_t *__restrict__ ev, int tg,
+                                                                     int bits, const uint32_t *__restrict__ w,
+                                                                     const uint32_t *__restrict__ psi,
+                                                                     const uint32_t *__restrict__ psi_inv,
+                                                                     uint32_t n_inv, uint32_t *__restrict__ bt,
+                                                                     uint32_t *__restrict__ last) {
+  namespace cg = cooperative_groups;
+  constexpr int n = 1 << L, NT = n / 8;
+  constexpr int ls = (L % 3) ? (L % 3) : 3, lt = n >> (L - ls + 1);  // the forward transform's last round
+  extern __shared__ uint32_t osm[];
+  cg::cluster_group cl = cg::this_cluster();
+  const int C = (int)cl.num_blocks(), k = (int)cl.block_rank();  // this CTA's digit
+  const int chain = blockIdx.x / C, o = chain >> 1, bar = chain & 1, half = n >> 1, g = threadIdx.x;
+  // parts[buffer][rank][slot]: every CTA pushes its share into every CTA's buffer (remote stores do not stall the
+  // thread, where remote loads would), and the buffers alternate by step, so one cluster barrier a step suffices
+  uint32_t *parts = osm + 2 * n;
+  int pb = 0;
+  const uint32_t mask = bits >= 32 ? 0xffffffffu : (1u << bits) - 1u;
+  const uint32_t *evo = ev + (size_t)o * n * n;
+  int ex = 0;
+  uint32_t x[8];
+  int e = gen_pow(half - 1, bar, n);
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    const int sl = 8 * g + m;
+    x[m] = mul_q(evo[(size_t)auto_slot(e, sl, n, L) * n + sl], n_inv);
+  }
+  for (int i = half - 2; i >= 0; --i) {
+    // this step's aggregate r_i (gathered from ev), loaded now so that its latency hides behind the transforms
+    e = gen_pow(i, bar, n);
+    uint32_t agg[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const int sl = 8 * g + m;
+      agg[m] = evo[(size_t)auto_slot(e, sl, n, L) * n + sl];
+    }
+    // inverse transform (without n^-1)
+    tail_round<L>(x, g, 0, 3, psi_inv);
+#pragma unroll
+    for (int s0 = 3; s0 < L; s0 += 3) {
+      const int r = (L - s0) < 3 ? (L - s0) : 3;
+      uint32_t *buf = osm + (ex++ & 1) * n;
+#pragma unroll
+      for (int m = 0; m < 8; ++m) buf[tail_swz(tail_index<L>(g, m, s0 - 3, 3))] = x[m];
+      __syncthreads();
+#pragma unroll
+      for (int gi = 0; gi < (8 >> r); ++gi) {
+        uint32_t *y = x + gi * (1 << r);
+#pragma unroll
+        for (int m = 0; m < (1 << r); ++m) y[m] = buf[tail_swz(tail_index<L>(gi * NT + g, m, s0, r))];
+        tail_round<L>(y, gi * NT + g, s0, r, psi_inv);
+      }
+    }
+    // this CTA's digit, in natural order, to the forward transform's first-round layout
+    {
+      constexpr int s0l = ((L - 1) / 3) * 3, rl = L - s0l;
+      uint32_t *buf = osm + (ex++ & 1) * n;
+#pragma unroll
+      for (int gi = 0; gi < (8 >> rl); ++gi)
+#pragma unroll
+        for (int m = 0; m < (1 << rl); ++m) {
+          const uint32_t v = mul_q(x[gi * (1 << rl) + m], n_inv);
+          buf[act_swz(tail_index<L>(gi * NT + g, m, s0l, rl))] =
+              (k < tg && bits * k < 32) ? (v >> (bits * k)) & mask : 0u;
+        }
+      __syncthreads();
+#pragma unroll
+      for (int b = 0; b < 8; ++b) x[b] = buf[act_swz(g + b * NT)];
+    }
+    fwd_round<L>(x, g, 3, 1, n >> 1, psi);
+#pragma unroll
+    for (int s0 = 3; s0 < L; s0 += 3) {
+      const int sr = (L - s0) < 3 ? (L - s0) : 3, t = n >> (s0 + 1), pt = n >> (s0 - 2);
+      uint32_t *buf = osm + (ex++ & 1) * n;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) buf[act_swz(fwd_pos<L>(g, 0, b, 3, pt))] = x[b];
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < 8 / (1 << sr); ++q)
+#pragma unroll
+        for (int b = 0; b < (1 << sr); ++b) x[q * (1 << sr) + b] = buf[act_swz(fwd_pos<L>(g, q, b, sr, t))];
+      fwd_round<L>(x, g, sr, 1 << s0, t, psi);
+    }
+    // bold_t[i][k], this CTA's share of the rotated sum, then the next r_i from every CTA's share
+    uint32_t *out = bt + (((size_t)chain * (half - 1) + i) * tg + k) * n;
+#pragma unroll
+    for (int q = 0; q < 8 / (1 << ls); ++q)
+#pragma unroll
+      for (int b = 0; b < (1 << ls); ++b) {
+        const int pos = fwd_pos<L>(g, q, b, ls, lt);
+        const uint32_t d = x[q * (1 << ls) + b];
+        if (k < tg) out[pos] = d;
+        const uint32_t v = k < tg ? mul_q(__ldg(w + k * n + auto_slot(e, pos, n, L)), d) : 0u;
+        for (int r = 0; r < C; ++r) cl.map_shared_rank(parts + ((size_t)pb * C + k) * n, r)[pos] = v;
+      }
+    cl.sync();  // every share has arrived in every CTA
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const int sl = 8 * g + m;
+      uint32_t acc = mul_q(agg[m], n_inv);
+      for (int r = 0; r < C; ++r) acc = add_q(acc, parts[((size_t)pb * C + r) * n + sl]);
+      x[m] = acc;
+    }
+    pb ^= 1;
+  }
+  cl.sync();  // no CTA exits while another may still write into its shared memory
+  if (k == 0)
+#pragma unroll
+    for (int m = 0; m < 8; ++m) last[(size_t)chain * n + 8 * g + m] = x[m];
 }
 
 // Per output (one CTA each): bold_t_hat = NTT(G^-1(rbar_0)); a_hat = INTT(r_0 + sum_k v[k] bold_t_hat[k]).  Writes

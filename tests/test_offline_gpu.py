@@ -42,8 +42,16 @@ def test_engine_over_the_oracle_scheme_state_decrypts(gpu, eng, client_mod, orac
         e.close()
 
 
-def test_device_offline_matches_the_oracle_restatement(gpu, client_mod, oracle, scheme_state):
+@pytest.mark.parametrize("variant", [{}, {"ALTO_OFFLINE_WALK8": "0"},
+                                     {"ALTO_OFFLINE_CLUSTER": "1", "ALTO_OFFLINE_ACT8": "0"}],
+                         ids=["register-walk", "cluster-walk", "single-cta-walk"])
+def test_device_offline_matches_the_oracle_restatement(gpu, client_mod, oracle, scheme_state, variant, monkeypatch):
+    """Every kernel variant of the set-up (the walk with register transforms on a 4-CTA cluster, the walk with
+    shared-memory transforms on a cluster, the single-CTA walk with the shared-memory hint transforms) gives the
+    oracle's values bit for bit."""
     from altopir_b200 import offline
+    for k, v in variant.items():
+        monkeypatch.setenv(k, v)
     st, p = scheme_state, scheme_state.p
     e = offline.blank_engine(p, st.db_col)
     try:
