@@ -140,14 +140,6 @@ class Ring:
             self._tables[t] = self.brv[k]
         return self._tables[t]
 
-    def tables(self):
-        """All n automorphism tables, table (t - 1) / 2 for odd t, as the engine's sw_pack_build reads them."""
-        return np.stack([self.table(t) for t in range(1, 2 * self.n, 2)]).astype(np.uint32)
-
-    def gen_pows(self):
-        """gen_pows[i] = 5^i mod 2n (src/packing.rs:1694-1703)."""
-        return np.array([pow(GEN, i, 2 * self.n) for i in range(self.n)], dtype=np.uint32)
-
 
 def gadget_invert(a, t=service.T_EXP_LEFT):
     """Base-2^9 digits of coefficient-form values in [0, Q): (..., n) -> (..., t, n), least significant first."""
@@ -191,15 +183,6 @@ def read_bits(buf, bit_off, width, count):
     bits = np.unpackbits(np.frombuffer(bytes(buf), dtype=np.uint8), bitorder="little")
     seg = bits[bit_off:bit_off + width * count].reshape(count, width).astype(np.uint64)
     return (seg << np.arange(width, dtype=np.uint64)).sum(axis=1).astype(np.uint64)
-
-
-def write_bits(buf, values, bit_off, width):
-    """OR `width`-bit values LSB first into the byte array buf from bit bit_off (write_arbitrary_bits)."""
-    values = np.asarray(values, dtype=np.uint64)
-    bits = ((values[:, None] >> np.arange(width, dtype=np.uint64)) & np.uint64(1)).astype(np.uint8).ravel()
-    allbits = np.unpackbits(buf, bitorder="little")
-    allbits[bit_off:bit_off + bits.size] |= bits
-    buf[:] = np.packbits(allbits, bitorder="little")
 
 
 def query_masks(rows, n):

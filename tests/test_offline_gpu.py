@@ -107,3 +107,32 @@ def test_device_offline_rejects_bad_arguments(gpu, svc):
                                          ctypes.byref(ms)) == 0 and ms.value > 0
     finally:
         e.close()
+
+
+def test_serving_loop_answers_the_scheme(gpu, client_mod, svc):
+    """The serving loop over an engine with the scheme's state: six clients each send two requests with the same
+    packing keys (the second is answered from the resident per-client table, without the pack), and every response
+    decrypts to its record."""
+    from altopir_b200 import offline, server as srv
+    p = svc.params(32768, 4096)
+    e, _ = offline.scheme_engine(p)
+    s = srv.Server(e, max_batch=8, queue_cap=64, slots=2)
+    try:
+        clients = [client_mod.Client(p, seed=70 + k) for k in range(6)]
+        keys = [c.packing_keys() for c in clients]
+        asks = [(k, (977 * k + 13 * r) % p.rows) for r in range(2) for k in range(6)]
+        done = []
+        for rnd in range(2):   # the second round's keys are resident by then
+            tickets = [(k, i, s.submit(clients[k].request(i, keys[k]))) for k, i in asks[6 * rnd:6 * rnd + 6]]
+            for k, i, t in tickets:
+                assert t >= 0
+                st, resp = s.wait(t, timeout_ms=30000)
+                assert st == 0
+                done.append((k, i, resp))
+        for k, i, resp in done:
+            assert np.array_equal(clients[k].decrypt(resp), svc.synthetic_record(i, p.record_bytes))
+        stats = s.stats()
+        assert stats["answered"] == 12 and stats["resident_hits"] >= 6
+    finally:
+        s.close()
+        e.close()
