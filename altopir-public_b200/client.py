@@ -13,7 +13,8 @@ randomness), which is not available here.  This module states the scheme's arith
 * the gadget with t = 4 digits of 9 bits (floor(log2ceil(Q) / t) + 1 bits a digit), the decomposition
   `gadget_invert_transposed_alloc` inverts (src/packing.rs:1468-1493);
 * secrets and errors from the discrete Gaussian of width 0.5 sqrt(2 pi) (sigma 0.5, `Xs = Xe = D(0.5)`,
-  src/scheme.rs:1-4, params.rs:102-104);
+  src/scheme.rs:1-4, params.rs:102-104), sampled by an exact 64-bit table from counter-based splitmix64 streams of
+  the client's secret seed (the reference draws them from OS entropy; the seed defaults to os.urandom);
 * public randomness (the query masks a_i and the packing masks w, v) from seeded splitmix64 streams instead of the
   reference's ChaCha20 streams; the server derives the same masks from the same seeds (`offline.py`).
 
@@ -22,6 +23,7 @@ OS entropy), but it has the reference's structure and distributions, and the eng
 the record asked for.
 """
 import math
+import os
 
 import numpy as np
 
@@ -45,12 +47,7 @@ _GAMMA = np.uint64(0x9E3779B97F4A7C15)
 def public_uniform(count, seed):
     """count values uniform in [0, Q) from the public stream `seed`: value i is the splitmix64 finaliser of
     seed + (i + 1) * gamma, mapped to [0, Q) by a multiply-high of its top 32 bits."""
-    with np.errstate(over="ignore"):
-        z = np.uint64(seed) + (np.arange(count, dtype=np.uint64) + np.uint64(1)) * _GAMMA
-        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
-        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
-        z = z ^ (z >> np.uint64(31))
-    return ((z >> np.uint64(32)) * np.uint64(Q)) >> np.uint64(32)
+    return ((splitmix_stream(seed, count) >> np.uint64(32)) * np.uint64(Q)) >> np.uint64(32)
 
 
 def _brv(n):
@@ -148,15 +145,35 @@ def gadget_invert(a, t=service.T_EXP_LEFT):
     return np.stack([(a >> np.uint64(GADGET_BITS * k)) & mask for k in range(t)], axis=-2)
 
 
-def gaussian(rng, shape, width=NOISE_WIDTH):
-    """Discrete Gaussian samples with Pr[x] proportional to exp(-pi x^2 / width^2), as values mod Q."""
-    sigma = width / math.sqrt(2 * math.pi)
-    tail = int(math.ceil(12 * sigma)) + 1
-    xs = np.arange(-tail, tail + 1)
-    cdf = np.cumsum(np.exp(-math.pi * xs.astype(np.float64) ** 2 / width ** 2))
-    cdf /= cdf[-1]
-    v = xs[np.searchsorted(cdf, rng.random(shape), side="right").clip(0, len(xs) - 1)]
-    return (v % Q).astype(np.uint64)
+# D(0.5): Pr[x] proportional to exp(-pi x^2 / (0.5 sqrt(2 pi))^2) = exp(-2 x^2).  CDT_THRESHOLDS[j] =
+# floor(2^64 Pr[X <= j - 4]) for j = 0..7 (computed at 60 decimal digits); a uniform 64-bit u gives
+# x = -4 + #{j : u >= CDT_THRESHOLDS[j]}, so Pr[x] is exact to 2^-64 and the support is [-4, 4] (the mass beyond +-4,
+# about 1e-14, goes to +-4).
+CDT_THRESHOLDS = np.array([0x2CDC8, 0x33738FE26B, 0x114B1F533EAC34, 0x1B51A6ACA1B1BEEB, 0xE4AE59535E4E4114,
+                           0xFFEEB4E0ACC153CB, 0xFFFFFFCC8C701D94, 0xFFFFFFFFFFFD3237], dtype=np.uint64)
+
+
+def splitmix_stream(seed, count):
+    """Value i of the stream `seed`: the splitmix64 finaliser of seed + (i + 1) * 0x9e3779b97f4a7c15."""
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + (np.arange(count, dtype=np.uint64) + np.uint64(1)) * _GAMMA
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def gaussian(seed, count):
+    """count samples of D(0.5) from the stream `seed`, as values mod Q."""
+    u = splitmix_stream(seed, count)
+    x = (u[:, None] >= CDT_THRESHOLDS[None, :]).sum(axis=1).astype(np.int64) - 4
+    return (x % Q).astype(np.uint64)
+
+
+def secret_stream(seed, purpose):
+    """The stream of a client's secret randomness for one purpose (0: s, 1: y's errors, 2: z's errors, 16 + j: the
+    errors of its j-th query)."""
+    with np.errstate(over="ignore"):
+        return int(np.uint64(seed) * np.uint64(0x9E3779B97F4A7C15) + np.uint64(purpose) * np.uint64(0xD1B54A32D192ED03))
 
 
 def rescale_q_to(a, out_mod):
@@ -209,17 +226,21 @@ class Client:
     engine's responses (spiral-rs Client + YClient, src/client.rs; service::new_request / decrypt_response)."""
 
     def __init__(self, p, seed=None, ring=None):
+        """seed: the client's secret seed (64 bits; from os.urandom when None -- the reference draws its secrets from
+        entropy).  Every secret value comes from counter-based streams of it, so a seeded client is reproducible
+        and the C++ client (include/altopir.hpp) with the same seed builds the same frames byte for byte."""
         self.p = p
         self.ring = ring or Ring(p.n)
-        self.rng = np.random.default_rng(seed)
-        self.s = gaussian(self.rng, p.n)                       # generate_secret_keys: sk_reg ~ D(0.5)
+        self.seed = int.from_bytes(os.urandom(8), "little") if seed is None else int(seed) & ((1 << 64) - 1)
+        self.queries = 0
+        self.s = gaussian(secret_stream(self.seed, 0), p.n)          # generate_secret_keys: sk_reg ~ D(0.5)
         self.s_hat = self.ring.ntt(self.s)
 
-    def _ksk_body(self, gen, mask):
+    def _ksk_body(self, gen, mask, purpose):
         """generate_ksk_body (src/packing.rs:2154-2177): -s * mask + e + tau_gen(s) * g, NTT form, (tg, n)."""
         r, q = self.ring, np.uint64(Q)
         tau_hat = r.ntt(r.automorph(self.s, gen))
-        e_hat = r.ntt(gaussian(self.rng, (self.p.tg, self.p.n)))
+        e_hat = r.ntt(gaussian(secret_stream(self.seed, purpose), self.p.tg * self.p.n).reshape(self.p.tg, self.p.n))
         g = np.array([pow(2, GADGET_BITS * k, Q) for k in range(self.p.tg)], dtype=np.uint64)[:, None]
         minus_s_mask = self.s_hat[None, :] * ((q - mask) % q) % q
         return (minus_s_mask + e_hat + tau_hat[None, :] * g % q) % q
@@ -228,8 +249,8 @@ class Client:
         """PackingKeys::init_full (src/packing.rs:1935-1984): y switches tau_5(s) to s under mask w, z switches
         tau_(2n-1)(s) (the conjugation) under mask v.  Returns the condensed (flat, NTT form) y and z."""
         w, v = packing_masks(self.p.n, self.p.tg)
-        y = self._ksk_body(GEN, w)
-        z = self._ksk_body(2 * self.p.n - 1, v)
+        y = self._ksk_body(GEN, w, 1)
+        z = self._ksk_body(2 * self.p.n - 1, v, 2)
         return y.reshape(-1), z.reshape(-1)
 
     def query(self, index):
@@ -240,7 +261,9 @@ class Client:
         if not 0 <= index < p.rows:
             raise ValueError("index out of range")
         a = query_masks(p.rows, p.n)
-        body = (r.intt(self.s_hat[None, :] * r.ntt(a) % q) + gaussian(self.rng, a.shape)) % q
+        err = gaussian(secret_stream(self.seed, 16 + self.queries), p.rows).reshape(a.shape)
+        self.queries += 1
+        body = (r.intt(self.s_hat[None, :] * r.ntt(a) % q) + err) % q
         body[index // p.n, index % p.n] = (body[index // p.n, index % p.n] + np.uint64(DELTA)) % q
         v = body.reshape(-1)
         return ((v << np.uint64(32)) + np.uint64(Q // 2)) // q & np.uint64(0xFFFFFFFF)

@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <fstream>
 #include <iostream>
+#include <iterator>
 #include <string>
 #include <vector>
 
@@ -164,9 +165,84 @@ static int gpu(const std::string &dir) {
   return failures;
 }
 
+// "client DIR": the client of seed / index in DIR/meta.txt ("rows record_bytes seed index") writes its frame to
+// DIR/frame.bin; if DIR/response.bin exists, the same client decrypts it into DIR/record.bin.
+static int client_files(const std::string &dir) {
+  size_t rows = 0, bytes = 0, index = 0;
+  uint64_t seed = 0;
+  std::ifstream meta(dir + "/meta.txt");
+  meta >> rows >> bytes >> seed >> index;
+  const Params p = params(rows, bytes);
+  client::Client c(p, seed);
+  const auto frame = c.request(index);
+  std::ofstream(dir + "/frame.bin", std::ios::binary).write((const char *)frame.data(), frame.size());
+  std::ifstream resp(dir + "/response.bin", std::ios::binary);
+  if (resp) {
+    std::vector<uint8_t> r((std::istreambuf_iterator<char>(resp)), std::istreambuf_iterator<char>());
+    const auto rec = c.decrypt(r.data(), r.size());
+    std::ofstream(dir + "/record.bin", std::ios::binary).write((const char *)rec.data(), rec.size());
+  }
+  CHECK(thrown([&] { c.decrypt(frame.data(), 10); }).find("expected") != std::string::npos);
+  return failures;
+}
+
+// "scheme ROWS BYTES": everything in C++ on the GPU -- an engine over the synthetic records generated on the
+// device, the scheme's offline set-up on the device, requests of four clients answered in one batch, decrypted.
+static int scheme(size_t rows, size_t bytes) {
+  init();
+  const Params p = params(rows, bytes);
+  const size_t outputs = p.instances();
+  std::vector<int8_t> ub(4 * bytes * p.count(), 0);
+  std::vector<std::vector<uint8_t>> pre(outputs, std::vector<uint8_t>(p.part_len(), 0));
+  std::vector<std::vector<uint64_t>> th(outputs, std::vector<uint64_t>(p.count(), 0));
+  std::vector<const uint8_t *> pp;
+  std::vector<const uint64_t *> tp;
+  for (size_t o = 0; o < outputs; ++o) {
+    pp.push_back(pre[o].data());
+    tp.push_back(th[o].data());
+  }
+  const auto inv = client::Ring(p.n).engine_inverse_table();
+  void *e = alto_engine_new_empty(rows, bytes, ub.data(), p.n, p.tg, pp.data(), p.part_len(), p.row1_off(), p.q1(),
+                                  p.q1_bits(), tp.data(), inv.data(), Q, 1);
+  CHECK(e != nullptr);
+  if (!e) return failures;
+  CHECK(alto_engine_fill_synthetic(e) == 0);
+  const double ms = client::prepare_offline(e, p);
+  CHECK(ms > 0);
+  const size_t idx[4] = {0, 7, rows / 2 + 3, rows - 1};
+  std::vector<client::Client> clients;
+  std::vector<std::vector<uint8_t>> frames, outs(4, std::vector<uint8_t>(response_len(p)));
+  std::vector<const uint8_t *> req;
+  std::vector<size_t> len;
+  std::vector<uint8_t *> outp;
+  for (int k = 0; k < 4; ++k) {
+    clients.emplace_back(p, 1000 + k);
+    frames.push_back(clients.back().request(idx[k]));
+  }
+  for (int k = 0; k < 4; ++k) {
+    req.push_back(frames[k].data());
+    len.push_back(frames[k].size());
+    outp.push_back(outs[k].data());
+  }
+  std::vector<int> status(4, -1);
+  std::array<double, 4> stage{};
+  CHECK(alto_answer(e, req.data(), len.data(), 4, outp.data(), status.data(), 0, stage.data()) == 4);
+  for (int k = 0; k < 4; ++k) {
+    CHECK(status[k] == 0);
+    CHECK(clients[k].decrypt(outs[k].data(), outs[k].size()) == synthetic::record(idx[k], bytes));
+  }
+  alto_engine_free(e);
+  std::cout << "offline set-up " << ms << " ms\n";
+  return failures;
+}
+
 int main(int argc, char **argv) {
   const std::string mode = argc > 1 ? argv[1] : "cpu";
-  const int f = mode == "gpu" && argc > 2 ? gpu(argv[2]) : cpu();
+  int f;
+  if (mode == "gpu" && argc > 2) f = gpu(argv[2]);
+  else if (mode == "client" && argc > 2) f = client_files(argv[2]);
+  else if (mode == "scheme" && argc > 3) f = scheme(std::stoull(argv[2]), std::stoull(argv[3]));
+  else f = cpu();
   if (f == 0) std::cout << "OK\n";
   return f == 0 ? 0 : 1;
 }

@@ -76,7 +76,11 @@ def test_request_has_the_reference_frame_layout(client_mod, svc):
     assert y.size == z.size == p.count and q.size == p.rows
     s = c.s.astype(np.int64)
     s = np.where(s > client_mod.Q // 2, s - client_mod.Q, s)
-    assert np.abs(s).max() <= 8 and 0.2 < (s != 0).mean() < 0.8      # D(0.5): mostly 0 and +-1
+    assert np.abs(s).max() <= 4 and 0.1 < (s != 0).mean() < 0.35     # D(0.5): 0 with probability 0.787
+    # a seeded client is reproducible, and its queries use fresh errors
+    c2 = client_mod.Client(p, seed=1)
+    assert np.array_equal(c2.request(7), frame)
+    assert not np.array_equal(c2.request(7), frame)
 
 
 def _records(oracle, idx, nbytes):
@@ -139,3 +143,17 @@ def test_offline_public_inputs_are_the_client_masks(client_mod, svc):
     assert q.shape == (p.rows // p.n, p.n) and np.array_equal((q + a) % client_mod.Q, np.zeros_like(a))
     w2, v2 = client_mod.packing_masks(p.n, p.tg)
     assert np.array_equal(w, w2) and np.array_equal(v, v2) and not np.array_equal(w, v)
+
+
+def test_gaussian_table_matches_d_half(client_mod):
+    """The 64-bit table gives Pr[x] = exp(-2 x^2) / Z to 2^-64; a million samples land within 5 sigma of it."""
+    import math
+    t = [int(v) for v in client_mod.CDT_THRESHOLDS]
+    z = sum(math.exp(-2 * x * x) for x in range(-6, 7))
+    for j, x in enumerate(range(-4, 4)):
+        want = sum(math.exp(-2 * y * y) for y in range(-6, x + 1)) / z
+        assert abs(t[j] / 2 ** 64 - want) < 1e-15
+    v = client_mod.gaussian(12345, 1_000_000).astype(np.int64)
+    v = np.where(v > client_mod.Q // 2, v - client_mod.Q, v)
+    for x, p in ((0, math.exp(0) / z), (1, math.exp(-2) / z), (-1, math.exp(-2) / z)):
+        assert abs((v == x).mean() - p) < 5 * math.sqrt(p * (1 - p) / v.size)

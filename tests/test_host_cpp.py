@@ -1,7 +1,9 @@
 """The C++ host layer (include/altopir.hpp), the C++ counterpart of the reference's Rust host side for the answer
 path: tests/cpp/test_host_api.cpp compiled here against the library.  On the CPU: parameter checks with the
 reference's messages, wire lengths, the request codec and its errors, synthetic records, TiledDb, Method.  On the GPU:
-an engine built through the C++ layer answers the golden case byte for byte."""
+an engine built through the C++ layer answers the golden case byte for byte.  The C++ client builds the Python
+client's frames and decrypts; on the GPU the whole scheme (device offline set-up, requests, decryption) runs
+through the C++ layer."""
 import os
 import subprocess
 
@@ -61,4 +63,31 @@ def test_modular_arithmetic_of_the_kernels(tmp_path):
                          capture_output=True, text=True)
     assert res.returncode == 0, res.stderr
     res = subprocess.run([out], capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0 and "OK" in res.stdout, res.stdout + res.stderr
+
+
+def test_cpp_client_builds_the_python_clients_frames_and_decrypts(host_api_bin, client_mod, oracle, scheme_state,
+                                                                  tmp_path):
+    """The C++ client (include/altopir.hpp, client::Client) and the Python client with the same seed build the same
+    frame byte for byte; the C++ client decrypts the response the oracle's engine gives over the scheme's state."""
+    p = scheme_state.p
+    seed, index = 0xC0FFEE, 1234
+    (tmp_path / "meta.txt").write_text(f"{p.rows} {p.record_bytes} {seed} {index}\n")
+    res = subprocess.run([host_api_bin, "client", str(tmp_path)], capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0 and "OK" in res.stdout, res.stderr
+    frame = np.fromfile(tmp_path / "frame.bin", dtype=np.uint8)
+    assert np.array_equal(frame, client_mod.Client(p, seed=seed).request(index))
+    _, status, out = oracle.answer(scheme_state, [frame])
+    assert list(status) == [0]
+    out[0].tofile(tmp_path / "response.bin")
+    res = subprocess.run([host_api_bin, "client", str(tmp_path)], capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0, res.stderr
+    rec = np.fromfile(tmp_path / "record.bin", dtype=np.uint8)
+    assert np.array_equal(rec, oracle.synthetic_record(index, p.record_bytes))
+
+
+@pytest.mark.gpu
+def test_cpp_scheme_round_trip_on_the_gpu(gpu, host_api_bin):
+    """Everything through the C++ layer: engine, device offline set-up, four clients' requests, decryption."""
+    res = subprocess.run([host_api_bin, "scheme", "32768", "4096"], capture_output=True, text=True, timeout=600)
     assert res.returncode == 0 and "OK" in res.stdout, res.stdout + res.stderr
