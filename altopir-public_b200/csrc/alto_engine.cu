@@ -567,6 +567,8 @@ struct Plan {
   int scan_n = 1;     // scan tiles along the limb columns (num_n / 2 when wide)
   int kb_chunk = 1;   // scan blocks per record chunk
   int bn = 16, num_n = 1;
+  int nw = 16;        // limb columns a pair-kernel tile computes: a multiple of 32 <= bn (bn: the kernel's template
+                      // width, a power of two), num_n tiles covering the batch's limb columns with least padding
   int scan_m = 0, scan_split = 1, scan_kb_per = 1, scan_kb = 0;
   int pack_m = 0, pack_kb = 0;
   int pairs_scan = 0, pairs_pack = 0;  // persistent grid of the pair kernels
@@ -597,7 +599,7 @@ Plan make_plan(const Engine *e, size_t slots) {
     return d;  // the smallest divisor of a chunk's blocks (a power of two here) that is >= kb_per
   };
   if (!p.pair) {
-    p.bn = pick_bn(limb_cols);
+    p.bn = p.nw = pick_bn(limb_cols);
     p.num_n = (int)((limb_cols + p.bn - 1) / p.bn);
     p.scan_m = (int)((e->cols + alto::kBM - 1) / alto::kBM);
     p.pack_m = (int)((4 * e->cols + alto::kBM - 1) / alto::kBM);
@@ -612,17 +614,39 @@ Plan make_plan(const Engine *e, size_t slots) {
     return p;
   }
   const int bn_cap = (tn && tn->bn_cap >= 32 && tn->bn_cap <= 256) ? tn->bn_cap : 256;
-  p.bn = 32;
-  while (p.bn < bn_cap && (size_t)p.bn < limb_cols) p.bn *= 2;
-  p.num_n = (int)((limb_cols + p.bn - 1) / p.bn);
+  // Power-of-two tiles (bn, the kernel's template width), or narrow ones: nw limb columns a tile, nw a multiple of 32
+  // (the pair kind::i8 MMA's N), as few tiles as the cap allows, each as narrow as covers the batch -- 144 limb
+  // columns (36 clients) in one 160-column tile instead of 256.  Narrow tiles are taken when they cut the columns
+  // computed by at least 30 %: at 8 GiB, 36 clients scanned in 1.50 ms against 1.80; at 2 x 160 against 2 x 256
+  // the two tied, and 224-column tiles (100 or 200 clients) ran 10-11 % slower than 256-column ones.
+  // ALTO_TILE_EXACT=0 never takes them, =1 always.
+  {
+    int bn2 = 32;
+    while (bn2 < bn_cap && (size_t)bn2 < limb_cols) bn2 *= 2;
+    const int n2 = (int)((limb_cols + bn2 - 1) / bn2);
+    const int nn = (int)((limb_cols + bn_cap - 1) / bn_cap);
+    const int nw = (int)round_up((limb_cols + nn - 1) / nn, 32);
+    bool narrow = (long)nn * nw * 10 <= (long)n2 * bn2 * 7;
+    if (const char *v = getenv("ALTO_TILE_EXACT")) narrow = v[0] != '0';
+    if (narrow) {
+      p.num_n = nn;
+      p.nw = nw;
+      p.bn = 32;
+      while (p.bn < p.nw) p.bn *= 2;
+    } else {
+      p.bn = p.nw = bn2;
+      p.num_n = n2;
+    }
+  }
   p.scan_m = (int)((e->cols + 255) / 256);
   p.pack_m = (int)((4 * e->cols + 255) / 256);
   const int pairs = resident_pairs();
   // Wide scan units once the database spans several record chunks (its tiles then stream from HBM and cannot be
   // shared between two pairs through L2) and there are at least 512 limb columns; ALTO_SCAN_WIDE=0/1 overrides.
-  p.wide = p.bn == 256 && p.num_n >= 2 && e->nchunks > 1;
-  if (tn && tn->wide >= 0) p.wide = p.bn == 256 && p.num_n >= 2 && tn->wide == 1;
-  if (const char *w = getenv("ALTO_SCAN_WIDE")) p.wide = p.bn == 256 && p.num_n >= 2 && w[0] == '1';
+  const bool full = p.bn == 256 && p.nw == 256;  // wide units take two full 256-column sub-accumulators
+  p.wide = full && p.num_n >= 2 && e->nchunks > 1;
+  if (tn && tn->wide >= 0) p.wide = full && p.num_n >= 2 && tn->wide == 1;
+  if (const char *w = getenv("ALTO_SCAN_WIDE")) p.wide = full && p.num_n >= 2 && w[0] == '1';
   p.scan_n = p.wide ? (p.num_n + 1) / 2 : p.num_n;
   // Scan chunks: at most 256 blocks (exactness, as above), at least 8, and about twelve units per resident pair so
   // the persistent pairs finish together.
@@ -636,7 +660,7 @@ Plan make_plan(const Engine *e, size_t slots) {
   p.pairs_scan = (int)std::min<long>(pairs, tiles * p.scan_split);
   // Wide pack units (ALTO_PACK_WIDE=1): both 256-column tiles of the limb columns in one unit, so each packing-
   // matrix tile is read once (and the epilogue no longer overlaps the next unit's MMAs)
-  if (const char *w = getenv("ALTO_PACK_WIDE")) p.pack_wide = p.bn == 256 && p.num_n >= 2 && w[0] == '1';
+  if (const char *w = getenv("ALTO_PACK_WIDE")) p.pack_wide = full && p.num_n >= 2 && w[0] == '1';
   const long pack_n = p.pack_wide ? (p.num_n + 1) / 2 : p.num_n;
   p.pairs_pack = (int)std::min<long>(pairs, (long)p.pack_m * pack_n);
   return p;
@@ -669,6 +693,7 @@ bool launch_scan(const Engine *e, const Plan &p, const CUtensorMap &map_q, uint3
     g.err = err;
     g.b_keep = keep_b;
     g.kb_chunk = p.kb_chunk;
+    g.nw = p.nw;
     return dispatch_pair<alto::Epi::kScan>(p.bn, e->map_db, map_q, g,
                                            std::min(p.pairs_scan, g.num_units), st, p.wide);
   }
@@ -707,6 +732,7 @@ bool launch_pack(const Engine *e, const Plan &p, const CUtensorMap &map_y, uint3
     g.err = err;
     g.b_keep = keep_b;
     g.kb_chunk = 1;
+    g.nw = p.nw;
     return dispatch_pair<alto::Epi::kPack>(p.bn, e->map_ub, map_y, g, p.pairs_pack, st, p.pack_wide);
   }
   alto::GemmArgs g;
@@ -725,11 +751,11 @@ bool launch_pack(const Engine *e, const Plan &p, const CUtensorMap &map_y, uint3
   return dispatch_gemm<alto::Epi::kPack>(p.bn, e->map_ub, map_y, g, p.pack_m * p.num_n, st);
 }
 
-// Tensor maps of the two limb operands for plan p (B boxes are BN rows for the single-CTA kernels and BN/2 rows,
-// one half per CTA, for the pair kernels).
+// Tensor maps of the two limb operands for plan p (B boxes are BN rows for the single-CTA kernels and nw/2 rows,
+// one half of a tile per CTA, for the pair kernels).
 bool make_limb_maps(const Engine *e, const Plan &p, const uint8_t *qlimb, const uint8_t *ylimb, size_t bp,
                     CUtensorMap *map_q, CUtensorMap *map_y) {
-  const uint32_t box = (uint32_t)(p.pair ? p.bn / 2 : p.bn);
+  const uint32_t box = (uint32_t)(p.pair ? p.nw / 2 : p.bn);
   return make_map3(map_q, qlimb, e->chunk, 4 * (uint64_t)bp, e->nchunks, box) &&
          make_map(map_y, ylimb, e->count, 4 * (uint64_t)bp, e->count, box);
 }

@@ -56,6 +56,10 @@ struct PairArgs {
   int m_begin;      // first 256-row tile along A (a launch may cover a column group)
   int kb_begin = 0; // first 128-byte block of the reduction (a launch may cover a range of record chunks;
                     // kb_total is then the range's end)
+  int nw = 0;       // limb columns a tile computes: a multiple of 32 <= BN (0: BN).  The B boxes are nw/2 rows
+                    // (the tensor map's box), loaded from the tile's origin n nw, and the MMAs run N = nw, so a
+                    // batch whose limb columns are not a power of two neither loads nor multiplies padding columns
+                    // (NSUB = 1 only)
 };
 
 // Epilogue of 16 TMEM columns (4 clients x 4 limbs) for one accumulator row of the scan: row = database column.
@@ -105,6 +109,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
   volatile int *bail = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // the tile width: a multiple of 32 in [32, BN] (the host checks), BN with NSUB = 2
+  const int nw = (NSUB == 1 && args.nw >= 32 && args.nw <= BN && args.nw % 32 == 0) ? args.nw : BN;
   const uint32_t rank = cluster_ctarank();
   const bool leader = rank == 0;
   const int pair = blockIdx.x >> 1, pairs = gridDim.x >> 1;
@@ -149,6 +155,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
   if (warp == 0) {
     // ------------------------------------------------------------ TMA producer (both CTAs)
     if (lane == 0) {
+      // both CTAs' A tiles and B boxes of this stage: the B box is nw/2 rows (the host makes the map with that box)
+      const uint32_t stage_tx = 2u * (uint32_t)(S::kABytes + NSUB * (nw / 2) * kBK);
       const uint64_t pol_a = policy_evict_first();
       const uint64_t pol_b = args.b_keep ? policy_evict_last() : policy_evict_normal();
       const uint32_t full_leader0 = map_to_rank(full0, 0);
@@ -164,21 +172,21 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
             break;
           }
           const uint32_t sa = base_addr + s * S::kStageBytes, sb = sa + S::kABytes;
-          if (leader) mbar_arrive_expect_tx(full0 + 8 * s, 2 * S::kStageBytes);
+          if (leader) mbar_arrive_expect_tx(full0 + 8 * s, stage_tx);
           if constexpr (EPI == Epi::kScan) {
             const int kb = kb0 + i, z = kb / args.kb_chunk, x = (kb - z * args.kb_chunk) * kBK;
             tma_load_tile_pair(sa, &map_a, full_leader0 + 8 * s, kb, 2 * m + (int)rank, pol_a);
 #pragma unroll
             for (int t = 0; t < NSUB; ++t)
               tma_load_3d_pair(sb + t * (BN / 2) * kBK, &map_b, full_leader0 + 8 * s, x,
-                               (n * NSUB + t) * BN + (int)rank * (BN / 2), z, pol_b);
+                               (n * NSUB + t) * nw + (int)rank * (nw / 2), z, pol_b);
           } else {
             const int x = (kb0 + i) * kBK;
             tma_load_tile_pair(sa, &map_a, full_leader0 + 8 * s, kb0 + i, 2 * m + (int)rank, pol_a);
 #pragma unroll
             for (int t = 0; t < NSUB; ++t)
               tma_load_2d_pair(sb + t * (BN / 2) * kBK, &map_b, full_leader0 + 8 * s, x,
-                               (n * NSUB + t) * BN + (int)rank * (BN / 2), pol_b);
+                               (n * NSUB + t) * nw + (int)rank * (nw / 2), pol_b);
           }
         }
       }
@@ -193,7 +201,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
   } else if (warp == 1) {
     // ------------------------------------------------------------ MMA issuer (leader CTA only)
     if (leader && lane == 0) {
-      constexpr uint32_t idesc = idesc_pair_u8u8_s32(BN);
+      const uint32_t idesc = idesc_pair_u8u8_s32((uint32_t)nw);
       int g = 0, it = 0;
       bool stop = false;
       for (int u = pair; u < args.num_units && !stop; u += pairs, ++it) {
@@ -247,13 +255,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
       const bool row_ok = grow < args.rows_a;
       // 32 columns per TMEM load (one wait per 8 clients instead of per 4)
 #pragma unroll 1
-      for (int ch = 0; ch < NSUB * BN / 32; ++ch) {
+      for (int ch = 0; ch < NSUB * nw / 32; ++ch) {
         uint32_t r[32];
         tmem_ld32(taddr + ch * 32, r);
         tmem_wait_ld();
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          const int c0 = n * NSUB * (BN / 4) + ch * 8 + h * 4;
+          const int c0 = n * NSUB * (nw / 4) + ch * 8 + h * 4;
           if constexpr (EPI == Epi::kScan)
             scan_epilogue16(r + 16 * h, grow, row_ok, c0, args.clients, args.cols, args.out);
           else

@@ -43,7 +43,8 @@ PUBLISHED_QPS = {32768: (1986.3, "README bench, 1 GB, batch 128: 64.44 ms median
                  262144: (492.0, "README Results table, 8 GB"),
                  2097152: (70.2, "README Results table, 64 GB")}
 # The larger configurations measured beside the headline (rows, batch sizes, single queries timed for the plain path).
-SUB_CONFIGS = ((262144, (1, 128, 1024), 32), (2097152, (128, 1024), 8))
+# the 8 GiB uneven-batch sweep and the 64 GiB batches of the workload list (records, batch sizes, plain queries)
+SUB_CONFIGS = ((262144, (1, 7, 33, 128, 200, 512, 1024), 32), (2097152, (128, 1024), 8))
 
 
 def parse(argv=None):

@@ -249,6 +249,26 @@ def test_every_schedule_returns_identical_bytes(gpu, svc, eng, monkeypatch):
         e.close()
 
 
+def test_narrow_tiles_return_the_oracles_bytes(gpu, oracle, svc, eng, monkeypatch):
+    """The pair GEMMs' run-time tile width (multiples of 32 limb columns, ALTO_TILE_EXACT) against power-of-two
+    tiles and the oracle, for batches whose limb columns fall just above a power of two and for several tiles."""
+    p = svc.params(2048, 4096)
+    st = svc.SyntheticState.make(p, seed=51)
+    for b in (9, 33, 65, 72, 100, 200):
+        frames = svc.synthetic_requests(p, b, seed=52 + b)
+        outs = []
+        for exact in ("1", "0"):
+            monkeypatch.setenv("ALTO_TILE_EXACT", exact)
+            e = eng.Engine.from_state(st)
+            n, status, out = _answer(e, [frames[i] for i in range(b)])
+            assert n == b and (status == 0).all()
+            outs.append(out)
+            e.close()
+        assert np.array_equal(outs[0], outs[1]), b
+        r, ost, oout = oracle.answer(st, [frames[i] for i in (0, b // 2, b - 1)])
+        assert np.array_equal(outs[0][[0, b // 2, b - 1]], oout), b
+
+
 def test_record_count_off_the_tile_grid_matches_oracle(gpu, oracle, svc, eng):
     # 2112 records: the last 128-record block of the tiled database is half padding, which must read as zero.  The
     # service layer only takes powers of two (as the reference's does); the engine's C ABI takes any multiple of 64.
