@@ -10,7 +10,7 @@ randomness), which is not available here.  This module states the scheme's arith
   (`generate_automorph_tables_brute_force`, src/packing.rs:1082-1110) -- computed with the Cooley-Tukey /
   Gentleman-Sande pair of Longa and Naehrig (CANS 2016, Algorithms 1 and 2); psi is the smallest primitive 2n-th
   root of unity mod Q;
-* the gadget with t = 4 digits of 9 bits (floor(log2ceil(Q) / t) + 1 bits a digit), the decomposition
+* the gadget with t digits of floor(log2ceil(Q) / t) + 1 bits (9 bits for the scheme's t = 4), the decomposition
   `gadget_invert_transposed_alloc` inverts (src/packing.rs:1468-1493);
 * secrets and errors from the discrete Gaussian of width 0.5 sqrt(2 pi) (sigma 0.5, `Xs = Xe = D(0.5)`,
   src/scheme.rs:1-4, params.rs:102-104), sampled by an exact 64-bit table from counter-based splitmix64 streams of
@@ -33,7 +33,6 @@ Q = service.Q
 P = 256                                  # plaintext modulus p (src/scheme.rs:3)
 DELTA = Q // P                           # scale_k = modulus / pt_modulus (src/client.rs:307)
 NOISE_WIDTH = 0.5 * math.sqrt(2 * math.pi)
-GADGET_BITS = 9                          # 32 // t + 1 for t = 4
 GEN = 5                                  # generator of the packing automorphisms for gamma = n (src/packing.rs:1697)
 
 # public stream counters (the reference's SEED_0, W_SEED and V_SEED, src/scheme.rs:15-29)
@@ -138,11 +137,19 @@ class Ring:
         return self._tables[t]
 
 
+def gadget_bits(t):
+    """Bits of a gadget digit for t digits: floor(log2ceil(Q) / t) + 1 = floor(32 / t) + 1, one bit when t = 32
+    (spiral-rs get_bits_per); 9 for the scheme's t = 4."""
+    return 1 if t >= 32 else 32 // t + 1
+
+
 def gadget_invert(a, t=service.T_EXP_LEFT):
-    """Base-2^9 digits of coefficient-form values in [0, Q): (..., n) -> (..., t, n), least significant first."""
+    """Base-2^gadget_bits(t) digits of coefficient-form values in [0, Q): (..., n) -> (..., t, n), least significant
+    first (gadget_invert_transposed_alloc, src/packing.rs:1468-1493)."""
     a = np.asarray(a, dtype=np.uint64)
-    mask = np.uint64((1 << GADGET_BITS) - 1)
-    return np.stack([(a >> np.uint64(GADGET_BITS * k)) & mask for k in range(t)], axis=-2)
+    b = gadget_bits(t)
+    mask = np.uint64((1 << b) - 1)
+    return np.stack([(a >> np.uint64(b * k)) & mask if b * k < 64 else np.zeros_like(a) for k in range(t)], axis=-2)
 
 
 # D(0.5): Pr[x] proportional to exp(-pi x^2 / (0.5 sqrt(2 pi))^2) = exp(-2 x^2).  CDT_THRESHOLDS[j] =
@@ -241,7 +248,8 @@ class Client:
         r, q = self.ring, np.uint64(Q)
         tau_hat = r.ntt(r.automorph(self.s, gen))
         e_hat = r.ntt(gaussian(secret_stream(self.seed, purpose), self.p.tg * self.p.n).reshape(self.p.tg, self.p.n))
-        g = np.array([pow(2, GADGET_BITS * k, Q) for k in range(self.p.tg)], dtype=np.uint64)[:, None]
+        bits = gadget_bits(self.p.tg)
+        g = np.array([pow(2, bits * k, Q) for k in range(self.p.tg)], dtype=np.uint64)[:, None]
         minus_s_mask = self.s_hat[None, :] * ((q - mask) % q) % q
         return (minus_s_mask + e_hat + tau_hat[None, :] * g % q) % q
 

@@ -286,7 +286,8 @@ inline std::optional<Request> decode_request(const Params &p, const uint8_t *inp
 // service::new_request / decrypt_response (src/service.rs:227-257) over src/client.rs and src/packing.rs, restated
 // without spiral-rs, as altopir-public_b200/client.py states it (the two build the same frames from the same seed):
 // the ring Z_Q[X]/(X^n + 1) with the negacyclic NTT whose slot j is the evaluation at psi^(2 brv(j) + 1), psi the
-// smallest primitive 2n-th root of unity (Longa-Naehrig transforms); gadget digits of 9 bits; secrets and errors from
+// smallest primitive 2n-th root of unity (Longa-Naehrig transforms); gadget digits of floor(32 / tg) + 1 bits (9 at
+// tg = 4); secrets and errors from
 // D(0.5) (Pr[x] ~ exp(-2 x^2)) by an exact 64-bit table over counter-based splitmix64 streams of the client's seed;
 // the public query and key masks from seeded streams that alto_engine_offline's caller uses too.
 namespace client {
@@ -294,7 +295,9 @@ namespace client {
 constexpr uint32_t kQ32 = 4294955009u;
 constexpr uint64_t kGamma = 0x9e3779b97f4a7c15ull;
 constexpr uint64_t QUERY_MASK_SEED = 0x5345454430ull, W_MASK_SEED = 0x5745454437ull, V_MASK_SEED = 0x5645454438ull;
-constexpr int GADGET_BITS = 9, GEN = 5, P = 256;
+constexpr int GEN = 5, P = 256;
+// bits of a gadget digit for t digits: floor(32 / t) + 1 (get_bits_per with log2ceil(Q) = 32), one bit at t = 32
+inline int gadget_bits(size_t t) { return t >= 32 ? 1 : (int)(32 / t) + 1; }
 constexpr uint64_t DELTA = Q / P;
 // floor(2^64 Pr[X <= j - 4]), j = 0..7, X ~ D(0.5)
 constexpr uint64_t kCdt[8] = {0x2CDC8ull,           0x33738FE26Bull,       0x114B1F533EAC34ull, 0x1B51A6ACA1B1BEEBull,
@@ -495,7 +498,7 @@ class Client {
     for (size_t k = 0; k < p_.tg; ++k) {
       for (size_t z = 0; z < n; ++z) e[z] = gaussian_at(secret_stream(seed_, purpose), k * n + z);
       ring_.ntt(e.data());
-      const uint32_t g = powq(2, (uint64_t)GADGET_BITS * k);
+      const uint32_t g = powq(2, (uint64_t)gadget_bits(p_.tg) * k);
       for (size_t z = 0; z < n; ++z)
         out[k * n + z] = addq(addq(mulq(s_hat_[z], subq(0, (uint32_t)(mask[k * n + z] % kQ32))), e[z]),
                               mulq(tau[z], g));

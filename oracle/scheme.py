@@ -14,15 +14,14 @@ What the reference computes with spiral-rs (absent here) is restated from the re
 * switch_prefix_row0 (src/modulus_switch.rs:136-147).
 
 The ring is Z_Q[X]/(X^n + 1) with the negacyclic NTT whose slot j is the evaluation at psi^(2 brv(j) + 1), psi
-the smallest primitive 2n-th root of unity, and the gadget has 4 digits of 9 bits.  Public masks come from the
-same seeded splitmix64 streams as the client's.  Parity with the reference's own offline values is unpinned (its
+the smallest primitive 2n-th root of unity, and the gadget has t digits of floor(32 / t) + 1 bits.  Public masks
+come from the same seeded splitmix64 streams as the client's.  Parity with the reference's own offline values is unpinned (its
 masks are ChaCha20 streams of spiral-rs); the restatement is pinned by decryption: responses of the reference's
 engine over this state decrypt to the records asked for.
 """
 import numpy as np
 
 Q = 4294955009
-GADGET_BITS = 9
 GEN = 5
 QUERY_MASK_SEED = 0x5345454430
 W_MASK_SEED = 0x5745454437
@@ -98,10 +97,12 @@ def perm(a):
 
 
 def gadget_digits(a, t):
-    """gadget_invert_transposed_alloc (src/packing.rs:1468-1493): base-2^9 digits, (..., n) -> (..., t, n)."""
+    """gadget_invert_transposed_alloc (src/packing.rs:1468-1493): digits of floor(32 / t) + 1 bits (get_bits_per
+    with log2ceil(Q) = 32; one bit when t = 32), (..., n) -> (..., t, n)."""
     a = np.asarray(a, dtype=np.uint64)
-    return np.stack([(a >> np.uint64(GADGET_BITS * k)) & np.uint64((1 << GADGET_BITS) - 1) for k in range(t)],
-                    axis=-2)
+    b = 1 if t >= 32 else 32 // t + 1
+    return np.stack([(a >> np.uint64(b * k)) & np.uint64((1 << b) - 1) if b * k < 64 else np.zeros_like(a)
+                     for k in range(t)], axis=-2)
 
 
 def hint(ring, db_col, masks):

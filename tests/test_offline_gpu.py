@@ -136,3 +136,29 @@ def test_serving_loop_answers_the_scheme(gpu, client_mod, svc):
     finally:
         s.close()
         e.close()
+
+
+@pytest.mark.parametrize("tg", [2, 8])
+def test_device_offline_at_other_key_counts(gpu, client_mod, oracle, svc, tg):
+    """tg = 2 and 8 gadget digits (17 and 5 bits; clusters of 2 and 8 CTAs in the walk) against the oracle bit for
+    bit; at tg = 8 the responses also decrypt (at tg = 2 the 17-bit digits leave too little noise margin)."""
+    from altopir_b200 import offline
+    from oracle.scheme import SchemeState
+    p = svc.Params(2048, 2048, tg=tg)
+    st = SchemeState(p, oracle.synthetic_db_col(p.rows, 0, p.record_bytes), oracle)
+    e = offline.blank_engine(p, st.db_col)
+    try:
+        _, out = offline.prepare(e, p, want=True)
+        for k in ("bold_t", "bold_t_bar", "that"):
+            assert np.array_equal(out[k][0].astype(np.uint64), getattr(st, k)[0]), k
+        assert np.array_equal(out["a_hat"][0].astype(np.uint64), st.a_hat[0])
+        idx = [5, 2000]
+        clients, frames = _clients(client_mod, p, idx, 80)
+        got = _answer(e, frames)
+        _, _, want = oracle.answer(st, frames)
+        assert np.array_equal(got, want)
+        if tg == 8:
+            for c, resp, i in zip(clients, got, idx):
+                assert np.array_equal(c.decrypt(resp), oracle.synthetic_record(i, p.record_bytes))
+    finally:
+        e.close()
