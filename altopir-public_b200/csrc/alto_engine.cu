@@ -1944,10 +1944,25 @@ int alto_engine_offline(void *p, const uint64_t *query, const uint64_t *w_mask, 
   // n = 2048: the act kernel with register transforms (ALTO_OFFLINE_ACT8=0 runs the shared-memory one)
   bool act8 = true;
   if (const char *v = getenv("ALTO_OFFLINE_ACT8")) act8 = v[0] != '0';
-  const size_t act8_smem = (2 + alto::kActCols) * n * sizeof(uint32_t);
-  if (n == 2048)
-    step(cudaFuncSetAttribute(alto::offline_act8_kernel<11>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)act8_smem));
+  // columns a CTA of the register-transform act kernel accumulates (ALTO_OFFLINE_ACTCOLS: 1, 2, 4 or 8).  Fewer
+  // columns keep less shared memory, so more CTAs share an SM: at 64 GiB the set-up took 736 ms with 8, 613 with 4,
+  // 586 with 2 and 582 with 1; at 1 GiB 31.4, 29.8, 29.4 and 29.5 ms.
+  int act_cols = 2;
+  if (const char *v = getenv("ALTO_OFFLINE_ACTCOLS")) {
+    const int c = atoi(v);
+    act_cols = c == 1 || c == 4 || c == 8 ? c : 2;
+  }
+  const size_t act8_smem = (2 + (size_t)act_cols) * n * sizeof(uint32_t);
+  if (n == 2048) {
+    step(cudaFuncSetAttribute(alto::offline_act8_kernel<11, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)((2 + 1) * n * sizeof(uint32_t))));
+    step(cudaFuncSetAttribute(alto::offline_act8_kernel<11, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)((2 + 2) * n * sizeof(uint32_t))));
+    step(cudaFuncSetAttribute(alto::offline_act8_kernel<11, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)((2 + 4) * n * sizeof(uint32_t))));
+    step(cudaFuncSetAttribute(alto::offline_act8_kernel<11, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)((2 + 8) * n * sizeof(uint32_t))));
+  }
   step(cudaFuncSetAttribute(alto::offline_walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)walk_smem));
   step(cudaFuncSetAttribute(alto::offline_finish_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)walk_smem));
   // the walk's cluster: one CTA per gadget digit, at most 8 (the portable cluster size); ALTO_OFFLINE_CLUSTER=1 runs
@@ -1975,9 +1990,18 @@ int alto_engine_offline(void *p, const uint64_t *query, const uint64_t *w_mask, 
     // the hint's query: NTT(perm(q_p)), without the n^-1 the coefficient-domain hint folds in
     alto::hint_query_kernel<<<(unsigned)polys, nt, n * sizeof(uint32_t)>>>(d_q, (int)n, d_psi, 1u, d_qhat);
     step(cudaGetLastError());
-    if (n == 2048 && act8) {
-      alto::offline_act8_kernel<11><<<(unsigned)(cols / alto::kActCols), 256, act8_smem>>>(
-          e->d_db, e->db_kbs, (int)polys, d_qhat, d_psi, d_act);
+    if (n == 2048 && act8 && act_cols == 1) {
+      alto::offline_act8_kernel<11, 1><<<(unsigned)cols, 256, act8_smem>>>(e->d_db, e->db_kbs, (int)polys, d_qhat,
+                                                                         d_psi, d_act);
+    } else if (n == 2048 && act8 && act_cols == 2) {
+      alto::offline_act8_kernel<11, 2><<<(unsigned)(cols / 2), 256, act8_smem>>>(e->d_db, e->db_kbs, (int)polys,
+                                                                               d_qhat, d_psi, d_act);
+    } else if (n == 2048 && act8 && act_cols == 4) {
+      alto::offline_act8_kernel<11, 4><<<(unsigned)(cols / 4), 256, act8_smem>>>(e->d_db, e->db_kbs, (int)polys,
+                                                                               d_qhat, d_psi, d_act);
+    } else if (n == 2048 && act8) {
+      alto::offline_act8_kernel<11, 8><<<(unsigned)(cols / 8), 256, act8_smem>>>(e->d_db, e->db_kbs, (int)polys,
+                                                                               d_qhat, d_psi, d_act);
     } else {
       alto::offline_act_kernel<<<(unsigned)(cols / alto::kActCols), 256, act_smem>>>(e->d_db, e->db_kbs, (int)n,
                                                                                     (int)polys, d_qhat, d_psi, d_act);

@@ -149,19 +149,20 @@ __device__ __forceinline__ int act_swz(int pos) { return pos ^ ((pos >> 5) & 31)
 
 // The act kernel with the transforms in registers: n / 8 threads, 8 values each, three stages per round and one
 // shared-memory exchange between rounds (double-buffered: one barrier an exchange), against a barrier per stage in
-// offline_act_kernel.  Same output.
-template <int L>
+// offline_act_kernel; ACOLS columns a CTA.  Same output.
+template <int L, int ACOLS>
 __global__ void __launch_bounds__((1 << L) / 8) offline_act8_kernel(const uint8_t *__restrict__ db, size_t kbs,
                                                                      int polys, const uint32_t *__restrict__ qhat,
                                                                      const uint32_t *__restrict__ psi,
                                                                      uint32_t *__restrict__ act) {
   constexpr int n = 1 << L, NT = n / 8;
+  static_assert(ACOLS >= 1 && n % ACOLS == 0, "columns per CTA");
   extern __shared__ uint32_t osm[];
   uint32_t *accs = osm + 2 * n;  // [column in CTA][position]
   const int g = threadIdx.x;
-  const size_t col0 = (size_t)blockIdx.x * kActCols;
+  const size_t col0 = (size_t)blockIdx.x * ACOLS;
   int ex = 0;  // exchanges so far: buffer ex & 1
-  for (int c = 0; c < kActCols; ++c) {
+  for (int c = 0; c < ACOLS; ++c) {
     const size_t col = col0 + c;
     const uint8_t *row = db + (col / 128) * kbs * 16384 + (col % 128) * 128;
     uint32_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -210,8 +211,8 @@ __global__ void __launch_bounds__((1 << L) / 8) offline_act8_kernel(const uint8_
   }
   __syncthreads();
   const size_t o = col0 / n, j0 = col0 % n;
-  for (int idx = threadIdx.x; idx < n * kActCols; idx += NT) {
-    const int s = idx / kActCols, c = idx - s * kActCols;
+  for (int idx = threadIdx.x; idx < n * ACOLS; idx += NT) {
+    const int s = idx / ACOLS, c = idx - s * ACOLS;
     act[(o * n + s) * n + j0 + c] = accs[c * n + (n - 1 - s)];
   }
 }
