@@ -94,7 +94,9 @@ struct Server {
   double loop_service_s = 0;  // loopback: simulated device time per batch
   std::vector<ServeSlot> slots;
   uint8_t *pool = nullptr;  // frame pool: entry i at pool + i * pitch (pinned for an engine)
-  std::vector<int> free_pool;
+  // free pool entries, handed out first in, first out: consecutive tickets get consecutive entries (the entries come
+  // back batch by batch in submission order), so a batch's frames upload in a few pitched copies, not one per frame
+  std::deque<int> free_pool;
   std::mutex mu;
   std::condition_variable cv;  // any change of queue, slots, in-flight or completed lists, or tickets
   std::deque<long long> queue;
@@ -559,7 +561,7 @@ bool server_start(Server *s, int nslots, size_t key_bytes) {
     s->pool = static_cast<uint8_t *>(malloc(s->queue_cap * s->pitch));
     if (!s->pool) return false;
   }
-  for (size_t i = 0; i < s->queue_cap; ++i) s->free_pool.push_back((int)(s->queue_cap - 1 - i));
+  for (size_t i = 0; i < s->queue_cap; ++i) s->free_pool.push_back((int)i);
   for (int i = 0; i < nslots; ++i) {
     ServeSlot &sl = s->slots[i];
     if (s->e) {
@@ -696,8 +698,8 @@ long long alto_server_submit(void *p, const uint8_t *frame, size_t len) {
     if (len != s->want) {  // status 1 at once: the frame never reaches a batch (src/amx_kernels.cpp:573)
       finish_ticket(s, *t, 1);
     } else {
-      t->pool = s->free_pool.back();
-      s->free_pool.pop_back();
+      t->pool = s->free_pool.front();
+      s->free_pool.pop_front();
     }
   }
   if (len != s->want) {
