@@ -97,6 +97,7 @@ struct Server {
   // free pool entries, handed out first in, first out: consecutive tickets get consecutive entries (the entries come
   // back batch by batch in submission order), so a batch's frames upload in a few pitched copies, not one per frame
   std::deque<int> free_pool;
+  bool pool_lifo = false;  // ALTO_SERVE_POOL=lifo: last in, first out (the earlier order, for comparison)
   std::mutex mu;
   std::condition_variable cv;  // any change of queue, slots, in-flight or completed lists, or tickets
   std::deque<long long> queue;
@@ -561,7 +562,8 @@ bool server_start(Server *s, int nslots, size_t key_bytes) {
     s->pool = static_cast<uint8_t *>(malloc(s->queue_cap * s->pitch));
     if (!s->pool) return false;
   }
-  for (size_t i = 0; i < s->queue_cap; ++i) s->free_pool.push_back((int)i);
+  if (const char *v = getenv("ALTO_SERVE_POOL")) s->pool_lifo = strcmp(v, "lifo") == 0;
+  for (size_t i = 0; i < s->queue_cap; ++i) s->free_pool.push_back((int)(s->pool_lifo ? s->queue_cap - 1 - i : i));
   for (int i = 0; i < nslots; ++i) {
     ServeSlot &sl = s->slots[i];
     if (s->e) {
@@ -698,8 +700,13 @@ long long alto_server_submit(void *p, const uint8_t *frame, size_t len) {
     if (len != s->want) {  // status 1 at once: the frame never reaches a batch (src/amx_kernels.cpp:573)
       finish_ticket(s, *t, 1);
     } else {
-      t->pool = s->free_pool.front();
-      s->free_pool.pop_front();
+      if (s->pool_lifo) {
+        t->pool = s->free_pool.back();
+        s->free_pool.pop_back();
+      } else {
+        t->pool = s->free_pool.front();
+        s->free_pool.pop_front();
+      }
     }
   }
   if (len != s->want) {
