@@ -162,3 +162,44 @@ def test_device_offline_at_other_key_counts(gpu, client_mod, oracle, svc, tg):
                 assert np.array_equal(c.decrypt(resp), oracle.synthetic_record(i, p.record_bytes))
     finally:
         e.close()
+
+
+@pytest.mark.skipif(not __import__("oracle.oracle", fromlist=["ref_methods"]).ref_methods(),
+                    reason="the reference engine needs AVX-512 (and its library in oracle/_ref)")
+def test_plain_small_config_against_the_reference_engine(gpu, eng, client_mod, oracle, svc):
+    """The plain small configuration: 2,048 synthetic records x 32 KB (64 MiB), the scheme's state built on the device,
+    one query of a seeded client; the GPU's response equals the reference engine's (src/amx_kernels.cpp compiled
+    unchanged) over the same state byte for byte, and decrypts to the record."""
+    from types import SimpleNamespace
+    from altopir_b200 import offline
+    from oracle.oracle import RefEngine, ref_methods
+    from oracle.scheme import prefix_row0, Ring
+    p = svc.params(2048, 32768)
+    db = oracle.synthetic_db_col(p.rows, 0, p.record_bytes)
+    e = offline.blank_engine(p, db)
+    try:
+        _, out = offline.prepare(e, p, want=True)
+        ring = client_mod.Ring(p.n)
+        tables = np.stack([Ring(p.n).table(t) for t in range(1, 2 * p.n, 2)]).astype(np.uint32)
+        gen_pows = np.array([pow(5, i, 2 * p.n) for i in range(p.n)], dtype=np.uint32)
+        bt = [np.ascontiguousarray(out["bold_t"][o], dtype=np.uint64) for o in range(p.instances)]
+        btb = [np.ascontiguousarray(out["bold_t_bar"][o], dtype=np.uint64) for o in range(p.instances)]
+        st = SimpleNamespace(
+            p=p, db_col=db, U=oracle.pack_build(bt, btb, tables, gen_pows, p.n // 2 - 1, p.tg, p.n),
+            that=[np.ascontiguousarray(out["that"][o], dtype=np.uint64) for o in range(p.instances)],
+            prefixes=[prefix_row0(out["a_hat"][o].astype(np.uint64), p.part_len) for o in range(p.instances)],
+            inv_table=client_mod.ntt_inverse_table(ring))
+        c = client_mod.Client(p, seed=0x5EED)
+        index = 1537
+        frame = c.request(index)
+        got = _answer(e, [frame])
+        ref = RefEngine(st)
+        try:
+            r, status, want, _ = ref.answer([frame], ref_methods()[0])
+        finally:
+            ref.close()
+        assert r == 1 and list(status) == [0]
+        assert np.array_equal(got[0], want[0])
+        assert np.array_equal(c.decrypt(got[0]), svc.synthetic_record(index, p.record_bytes))
+    finally:
+        e.close()
