@@ -203,3 +203,28 @@ def test_plain_small_config_against_the_reference_engine(gpu, eng, client_mod, o
         assert np.array_equal(c.decrypt(got[0]), svc.synthetic_record(index, p.record_bytes))
     finally:
         e.close()
+
+
+def test_column_shards_build_their_own_scheme_state(gpu, client_mod, svc):
+    """Column sharding with the scheme's state: each shard engine (a contiguous range of outputs) runs the device
+    set-up over its own columns only; the shards' parts, concatenated in output order, equal the full engine's
+    response byte for byte and decrypt to the record."""
+    from altopir_b200 import offline
+    p = svc.params(32768, 8192)                                   # 4 outputs
+    full, _ = offline.scheme_engine(p)
+    shards = []
+    try:
+        for c0, c1 in ((0, 2048), (2048, 8192)):                  # shards of 1 and 3 outputs
+            ps = svc.Params(p.rows, c1 - c0)
+            e, _ = offline.scheme_engine(ps, np.ascontiguousarray(svc.synthetic_db_col(p.rows, c1 - c0, col0=c0)))
+            shards.append(e)
+        c = client_mod.Client(p, seed=91)
+        frame = c.request(30001)
+        want = _answer(full, [frame])[0]
+        got = np.concatenate([_answer(e, [frame])[0] for e in shards])
+        assert np.array_equal(got, want)
+        assert np.array_equal(c.decrypt(got), svc.synthetic_record(30001, p.record_bytes))
+    finally:
+        full.close()
+        for e in shards:
+            e.close()
