@@ -306,7 +306,8 @@ int alto_hint_ring(void *engine, const uint64_t *query, uint64_t *out, int perm_
  * ms (optional) receives the device time of the set-up.  Waits for the engine's batches in flight (a serving loop
  * must not run on the engine meanwhile); allocates about 4 n cols + 4 tg n cols + 12 records bytes of device scratch
  * for the call (1.3 GB at 32 KB records, n = 2048, tg = 4).  0, -1 for bad arguments or an unsupported
- * configuration, -4 for a device failure. */
+ * configuration (the engine is untouched), -4 for a device failure (the engine's packing state is then undefined:
+ * call again or free it). */
 int alto_engine_offline(void *engine, const uint64_t *query, const uint64_t *w_mask, const uint64_t *v_mask,
                         uint32_t *bold_t, uint32_t *bold_t_bar, uint32_t *that, uint32_t *a_hat, double *ms);
 
