@@ -72,6 +72,7 @@ struct Resident {
 // + download, total.
 constexpr int kLogFields = 10;
 constexpr size_t kLogRows = 65536;
+constexpr int kBaseSlots = 2;  // contexts that take any batch; the others wait for a deep queue (Server::deep_queue)
 
 struct ServeSlot {
   Batch b;
@@ -103,6 +104,9 @@ struct Server {
   std::deque<long long> queue;
   std::unordered_map<long long, Ticket> tickets;
   std::deque<int> free_slots, inflight, completed;
+  // contexts beyond the first kBaseSlots take a batch only while the queue holds at least deep_queue frames: a
+  // third concurrent full-database scan raises every batch's latency below saturation and pays only at it
+  size_t deep_queue = 0;
   long long next_id = 0;
   bool stop = false, batcher_done = false;
   std::thread batcher, completer;
@@ -368,18 +372,24 @@ void batcher_loop(Server *s) {
     int si = -1;
     {
       std::unique_lock<std::mutex> lk(s->mu);
+      // a free context that may take the queue's frames now: the lowest-numbered one (see deep_queue)
+      auto pick = [&]() -> int {
+        int best = -1;
+        for (int d : s->free_slots)
+          if ((d < kBaseSlots || s->queue.size() >= s->deep_queue) && (best < 0 || d < best)) best = d;
+        return best;
+      };
       s->cv.wait(lk, [&] {
-        return (s->stop && s->queue.empty()) || !s->completed.empty() ||
-               (!s->queue.empty() && !s->free_slots.empty());
+        return (s->stop && s->queue.empty()) || !s->completed.empty() || (!s->queue.empty() && pick() >= 0);
       });
       while (!s->completed.empty()) {
         done_slots.push_back(s->completed.front());
         s->completed.pop_front();
       }
       if (done_slots.empty() && s->queue.empty()) break;  // stopping and drained
-      if (!s->queue.empty() && !s->free_slots.empty()) {
-        si = s->free_slots.front();
-        s->free_slots.pop_front();
+      if (!s->queue.empty() && pick() >= 0) {
+        si = pick();
+        s->free_slots.erase(std::find(s->free_slots.begin(), s->free_slots.end(), si));
         const size_t n = std::min(s->queue.size(), s->max_batch);
         for (size_t i = 0; i < n; ++i) {
           ids.push_back(s->queue.front());
@@ -546,6 +556,9 @@ size_t table_capacity(const Engine *e, size_t key_bytes) { return key_bytes / (e
 bool server_start(Server *s, int nslots, size_t key_bytes) {
   s->pitch = round_up(s->want, 64);
   s->slots.resize(nslots);
+  // contexts beyond the first two wait for half a maximum batch in the queue (ALTO_SERVE_DEEP: frames, 0 = always)
+  s->deep_queue = std::max<size_t>(1, s->max_batch / 2);
+  if (const char *v = getenv("ALTO_SERVE_DEEP")) s->deep_queue = (size_t)strtoull(v, nullptr, 10);
   if (s->e) {
     ALTO_CK(cudaHostAlloc(&s->pool, s->queue_cap * s->pitch, cudaHostAllocDefault));
     s->ybytes = 4 * s->e->count;
