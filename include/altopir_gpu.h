@@ -188,6 +188,8 @@ int alto_answer_device_noalloc(void *engine, const uint8_t *d_req, size_t req_st
  * a batcher thread takes whatever is queued, up to max_batch, as soon as one of `slots` device batch contexts (1..8)
  * is free -- it never holds a request back to fill a batch, and frames that arrive while every context is busy join
  * the next batch -- and answers it on that context's stream, so up to `slots` batches upload and compute at once.
+ * Contexts beyond the first two take a batch only while at least max_batch / 2 frames are queued (environment
+ * ALTO_SERVE_DEEP: frames, 0 = always): a third concurrent full-database scan pays only at saturation.
  * Per-client state in HBM: the pack product beta = y U of a client's packing keys y depends on nothing else, so the
  * loop keeps it in a resident table of key_bytes / (cols * 4) rows.  A frame whose y keys equal, byte for byte, those
  * of a resident client skips the pack GEMM and gathers its row; a new client is admitted to a free row, or to the
