@@ -228,3 +228,48 @@ def test_column_shards_build_their_own_scheme_state(gpu, client_mod, svc):
         full.close()
         for e in shards:
             e.close()
+
+
+def test_device_path_graphs_and_lanes_see_the_new_state(gpu, client_mod, svc):
+    """Graphs captured and lanes made before the set-up replay over the state it writes in place: the engine answers
+    device-resident frames of four clients through two lanes with graph replay, then runs alto_engine_offline, and
+    the same replayed path now returns responses that decrypt (and equal alto_answer's)."""
+    import torch
+    from altopir_b200 import offline
+    p = svc.params(32768, 4096)
+    e = offline.blank_engine(p)
+    try:
+        idx = [3, 4096, 20000, 32767]
+        clients, frames = _clients(client_mod, p, idx, 300)
+        ql, rl, b = e.request_len(), e.response_len(), len(frames)
+        stride = (7 + ql + 15) // 16 * 16
+        slots = torch.zeros((b, stride), dtype=torch.uint8, device="cuda")
+        slots[:, 7:7 + ql] = torch.from_numpy(np.stack(frames)).cuda()
+        e.set_graphs(True)
+        e.set_lanes(2)
+        stream = torch.cuda.ExternalStream(e.stream())
+
+        def device_answer():
+            out = torch.full((b, rl), 0x11, dtype=torch.uint8, device="cuda")
+            st = torch.full((b,), -1, dtype=torch.int32, device="cuda")
+            torch.cuda.synchronize()
+            for _ in range(2):   # both lanes capture and replay
+                e.enqueue_device(slots.data_ptr(), stride, b, out.data_ptr(), rl, st.data_ptr())
+            e.fence()
+            with torch.cuda.stream(stream):
+                o, s = out.clone(), st.clone()
+            stream.synchronize()
+            e.sync()
+            return o.cpu().numpy(), s.cpu().numpy()
+
+        before, _ = device_answer()
+        offline.prepare(e, p)
+        after, st = device_answer()
+        assert list(st) == [0] * b and not np.array_equal(before, after)
+        assert np.array_equal(after, _answer(e, frames))
+        for c, resp, i in zip(clients, after, idx):
+            assert np.array_equal(c.decrypt(resp), svc.synthetic_record(i, p.record_bytes))
+        e.set_lanes(1)
+        e.set_graphs(False)
+    finally:
+        e.close()
