@@ -615,18 +615,21 @@ Plan make_plan(const Engine *e, size_t slots) {
   }
   const int bn_cap = (tn && tn->bn_cap >= 32 && tn->bn_cap <= 256) ? tn->bn_cap : 256;
   // Power-of-two tiles (bn, the kernel's template width), or narrow ones: nw limb columns a tile, nw a multiple of 32
-  // (the pair kind::i8 MMA's N), as few tiles as the cap allows, each as narrow as covers the batch -- 144 limb
-  // columns (36 clients) in one 160-column tile instead of 256.  Narrow tiles are taken when they cut the columns
-  // computed by at least 30 %: at 8 GiB, 36 clients scanned in 1.50 ms against 1.80; at 2 x 160 against 2 x 256
-  // the two tied, and 224-column tiles (100 or 200 clients) ran 10-11 % slower than 256-column ones.
-  // ALTO_TILE_EXACT=0 never takes them, =1 always.
+  // (the pair kind::i8 MMA's N), as few tiles as the cap allows, each as narrow as covers the batch.  Narrow tiles are
+  // taken when they cut the columns computed by at least 20 %, which leaves out 224-column tiles.  Measured at 8 GiB
+  // (scan ms, power-of-two / narrow): 36 clients 1.83 / 1.54 on one 160-column tile (1.60 on 192); 48 clients
+  // 1.82 / 1.66 on 192; 136 clients 6.13 / 4.63 on 3 x 192; 70 clients 2.81 / 2.92 on 2 x 160 (the one loss);
+  // 224-column tiles (100 or 200 clients) ran 10-11 % slower than 256-column ones.  ALTO_TILE_EXACT=0 never takes
+  // narrow tiles, =1 always; ALTO_TILE_ALIGN=64 rounds their width to a multiple of 64.
   {
     int bn2 = 32;
     while (bn2 < bn_cap && (size_t)bn2 < limb_cols) bn2 *= 2;
     const int n2 = (int)((limb_cols + bn2 - 1) / bn2);
     const int nn = (int)((limb_cols + bn_cap - 1) / bn_cap);
-    const int nw = (int)round_up((limb_cols + nn - 1) / nn, 32);
-    bool narrow = (long)nn * nw * 10 <= (long)n2 * bn2 * 7;
+    int align = 32;
+    if (const char *v = getenv("ALTO_TILE_ALIGN")) align = atoi(v) == 64 ? 64 : 32;
+    const int nw = (int)std::min<size_t>(round_up((limb_cols + nn - 1) / nn, align), (size_t)bn_cap);
+    bool narrow = (long)nn * nw * 10 <= (long)n2 * bn2 * 8;
     if (const char *v = getenv("ALTO_TILE_EXACT")) narrow = v[0] != '0';
     if (narrow) {
       p.num_n = nn;
